@@ -1,0 +1,256 @@
+/*
+ * lipika_cuda.h — C ABI of the B200 (sm_100a) IQ-generation backend.
+ *
+ * The boundary replaces the per-chunk transmitter fan-out of the reference
+ * and everything after the transmitter sum, src/pipeline.rs:943-983:
+ *   gated_contribution -> accumulate_reporting_occlusion (channel/mod.rs:164-271)
+ *   fixed-order reduction                                 (pipeline.rs:966-977)
+ *   add_awgn_at_power                                      (channel/mod.rs:323-334)
+ *   RxChain::apply_post_sum                                (rx/mod.rs:142-146)
+ * The chunk loop, the clock stream and the sinks stay in the host.
+ *
+ * Conventions (all entry points):
+ *   - plain C types and pointers only; no CUDA or torch types cross the ABI;
+ *   - every call returns an lpk_status (0 = OK, negative = error) and never
+ *     aborts or exits; lpk_last_error() holds a message for the last failure;
+ *   - host pointers are borrowed for the duration of the call only; the
+ *     library copies what it keeps into memory owned by the lpk_ctx;
+ *   - one lpk_ctx per host thread: calls on different contexts are
+ *     thread-safe, calls on one context must be serialised (the reference
+ *     calls generate_band concurrently from rayon workers,
+ *     src/pipeline.rs:513-535, each with its own state).
+ */
+#ifndef LIPIKA_CUDA_H
+#define LIPIKA_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "lipika_scene.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t lpk_status;
+#define LPK_OK 0
+#define LPK_EINVAL (-1)     /* bad descriptor, NaN or out-of-range configuration */
+#define LPK_ENOMEM (-2)     /* host or device allocation failed */
+#define LPK_ECUDA (-3)      /* a CUDA call failed; lpk_last_error() has its string */
+#define LPK_ETIMEDOUT (-4)  /* a bounded device wait gave up */
+#define LPK_ENOCONV (-5)    /* an emission solve did not converge */
+#define LPK_ENOTSUP (-6)    /* feature outside this backend (TLE, RINEX, LNAV) */
+
+typedef struct lpk_ctx lpk_ctx;
+typedef struct lpk_cf32 { float re, im; } lpk_cf32;
+
+/* ------------------------------------------------------------------ */
+/* Context                                                             */
+/* ------------------------------------------------------------------ */
+/* Create a context bound to CUDA device `device` (own stream + buffers).
+ * Replaces: Backend::Cpu selection, src/backend/mod.rs:16-18. */
+lpk_status lpk_ctx_create(lpk_ctx **out, int32_t device);
+void lpk_ctx_destroy(lpk_ctx *ctx);
+/* Message of the last failed call on this context ("" if none). */
+const char *lpk_last_error(const lpk_ctx *ctx);
+/* Message of the last failure that happened before a context existed. */
+const char *lpk_global_last_error(void);
+/* Library version string. */
+const char *lpk_version(void);
+
+/* ------------------------------------------------------------------ */
+/* Kernel-level boundary: transmitters as already-built tables          */
+/* ------------------------------------------------------------------ */
+enum { LPK_TX_TRAJ_STATIONARY = 0, LPK_TX_TRAJ_PRECOMPUTED = 1 };
+
+/* One transmitter as the reference's host holds it after prepare():
+ * AnyTrajectory::{Stationary, Precomputed} (geometry/mod.rs:25-31,
+ * precomputed.rs:157-172) + a SignalModel (src/signal/) + EIRP.
+ * Tables are host pointers, copied by lpk_scene_upload. */
+typedef struct lpk_tx_desc {
+    int32_t traj_kind;          /* LPK_TX_TRAJ_* */
+    int32_t sig_kind;           /* LPK_SIG_* (lipika_scene.h) */
+    double stationary_ecef[3];
+    double grid_t0_unix;        /* PrecomputedTrajectory::t0_unix */
+    double grid_dt_s;           /* ::dt_s */
+    int64_t grid_n;             /* ::n */
+    const double *grid_xyz;     /* (3, grid_n) axis-major, as ndarray holds it */
+    double carrier_hz;          /* SignalModel::carrier_hz */
+    double tx_power_w;          /* 10^(dBW/10), pipeline.rs:338 */
+    /* framed kinds (bpsk, ook, qam16) and ca_code */
+    double epoch_rel_s;         /* symbol/chip-0 tag, scene-epoch relative */
+    double rate_hz;             /* bit or symbol rate (framed kinds) */
+    int32_t has_repeat;         /* repeat_from is Some */
+    int32_t nav_kind;           /* ca_code: LPK_NAV_* */
+    int64_t repeat_from;
+    int64_t n_sym;              /* frame length */
+    const int8_t *pm_bits;      /* bpsk: n_sym values ±1 */
+    const uint8_t *ook_bits;    /* ook: n_sym values 0/1 */
+    const lpk_cf32 *symbols;    /* qam16: n_sym constellation points */
+    const int8_t *chips;        /* ca_code: 1023 values ±1 */
+    uint64_t nav_seed;          /* dummy nav: folded seed (ca_code.rs:148-149) */
+    const int8_t *nav_bits;     /* full nav: nav_n values ±1 */
+    int64_t nav_n;
+    /* cw */
+    double cw_offset_hz;
+    double cw_phase0;           /* anchored phase (cw.rs:22-34) */
+    int32_t cw_anchored;
+    /* burst gate (gate.rs:27-34) */
+    int32_t has_gate;
+    double gate_period_s;
+    double gate_phase_s;
+    int32_t gate_n;
+    int32_t reserved;
+    const double *gate_on;      /* gate_n (start, end) pairs */
+} lpk_tx_desc;
+
+/* Upload the scene's transmitters (replaces the host-side Vec<Transmitter>
+ * the fan-out reads, src/pipeline.rs:297-342). Replaces any earlier upload. */
+lpk_status lpk_scene_upload(lpk_ctx *ctx, const lpk_tx_desc *tx, int32_t n_tx);
+
+enum { LPK_CLOCK_HOST = 0, LPK_CLOCK_DETERMINISTIC = 1, LPK_CLOCK_DEVICE_WALK = 2 };
+enum { LPK_RX_STATIONARY = 0, LPK_RX_PER_SAMPLE = 1 };
+enum { LPK_POST_GAIN = 0, LPK_POST_NONLINEARITY = 1, LPK_POST_ADC = 2 };
+enum { LPK_SOLVER_REFERENCE = 0, LPK_SOLVER_SPLIT = 1 };
+
+typedef struct lpk_post_op {
+    int32_t kind;               /* LPK_POST_* */
+    uint32_t bits;              /* adc */
+    double param;               /* gain_db | iip3_w | full_scale_v */
+} lpk_post_op;
+
+/* One (receiver, band) work unit's per-chunk parameters
+ * (generate_band's locals, src/pipeline.rs:853-905). */
+typedef struct lpk_band_desc {
+    double epoch_unix;          /* scene epoch */
+    double fs_hz;               /* band sample rate */
+    double lo_hz;               /* band LO */
+    double noise_power_w;       /* AWGN power; <= 0 disables noise */
+    uint64_t noise_seed;        /* noise_seed(base, work_idx), pipeline.rs:828 */
+    int32_t rx_kind;            /* LPK_RX_* */
+    int32_t clock_mode;         /* LPK_CLOCK_* */
+    double rx_ecef[3];          /* stationary receiver */
+    /* clock (NodeClockSpec) for DETERMINISTIC / DEVICE_WALK modes */
+    double clock_offset_s;
+    double clock_y0;
+    double clock_allan_1s;
+    double clock_master_rate_hz;
+    uint64_t clock_seed;        /* clock_seed(base, r_idx), pipeline.rs:825 */
+    /* antenna (Antenna, rx/mod.rs:41-58) */
+    int32_t has_antenna;
+    int32_t has_cutoff;
+    double ant_peak_dbi, ant_horizon_dbi, ant_fb_db, ant_cutoff_deg;
+    /* post-sum chain (RxChain::post_sum, rx/mod.rs:117-146) */
+    int32_t n_post;
+    int32_t solver;             /* LPK_SOLVER_* */
+    lpk_post_op post[3];
+} lpk_band_desc;
+
+/* One chunk of one band through the fan-out, Σ, AWGN and rx chain.
+ * Replaces src/pipeline.rs:943-983 for the chunk [i0, i0 + n).
+ *   active_tx  : indices into the uploaded transmitters, in band order
+ *                (the band-overlap gate's `active`, pipeline.rs:882-891)
+ *   delta_t    : n clock offsets Δt (host), required for LPK_CLOCK_HOST
+ *   rx_pos3n   : (3, n) receiver ECEF per sample (host), LPK_RX_PER_SAMPLE
+ *   out        : n complex64 samples (host)
+ *   unoccluded : n_active flags OR-ed with "non-zero antenna gain for at
+ *                least one sample" (accumulate_reporting_occlusion's
+ *                return value, channel/mod.rs:204-207); may be NULL. */
+lpk_status lpk_band_chunk(lpk_ctx *ctx, const lpk_band_desc *band, const int32_t *active_tx,
+                          int32_t n_active, int64_t i0, int64_t n, const double *delta_t,
+                          const double *rx_pos3n, lpk_cf32 *out, uint8_t *unoccluded);
+
+/* Same as lpk_band_chunk, but every array is DEVICE memory and the work is
+ * only enqueued on the context's stream (call lpk_sync to wait). Used by
+ * hosts that keep inputs and outputs resident in HBM. */
+lpk_status lpk_band_chunk_device(lpk_ctx *ctx, const lpk_band_desc *band, const int32_t *active_tx,
+                                 int32_t n_active, int64_t i0, int64_t n, const double *d_delta_t,
+                                 const double *d_rx_pos3n, lpk_cf32 *d_out, uint8_t *d_unoccluded);
+lpk_status lpk_sync(lpk_ctx *ctx);
+
+/* Per-transmitter emission solve (channel/mod.rs:106-121,
+ * solve_emission_times): `iterations` fixed-point steps from t - 70 ms.
+ * All arrays host memory, obs3n is (3, n) axis-major. */
+lpk_status lpk_solve_emission_times(lpk_ctx *ctx, int32_t tx, const double *obs3n,
+                                    const double *t_rel_utc, int64_t n, double epoch,
+                                    int32_t iterations, double *t_emit, double *ranges);
+
+/* One transmitter's contribution alone (channel/mod.rs:278-298,
+ * transmitter_contribution_at_receiver) for the band's chunk; optional
+ * per-sample carrier phase reduced to [-pi, pi) (phase_out, may be NULL). */
+lpk_status lpk_tx_contribution(lpk_ctx *ctx, const lpk_band_desc *band, int32_t tx, int64_t i0,
+                               int64_t n, const double *delta_t, const double *rx_pos3n,
+                               lpk_cf32 *out, double *phase_out, double *t_emit_out,
+                               double *range_out);
+
+/* AWGN-free rx chain alone on n samples in place (RxChain::apply_post_sum,
+ * src/rx/mod.rs:142-146): the band's post ops on caller-supplied f32 IQ,
+ * so ADC codes can be compared on identical inputs. Host memory. */
+lpk_status lpk_rx_chain_apply(lpk_ctx *ctx, const lpk_band_desc *band, lpk_cf32 *iq, int64_t n);
+
+/* ------------------------------------------------------------------ */
+/* Host-level mirror of src/pipeline.rs (scene -> per-band streams)     */
+/* ------------------------------------------------------------------ */
+typedef struct lpk_scene lpk_scene;
+
+/* prepare() (src/pipeline.rs:801-819): build every transmitter's
+ * trajectory table and signal tables from the scene description, check
+ * them, and upload them to ctx. The scene keeps a borrowed ctx pointer.
+ * With ctx == NULL the tables are built and checked but not uploaded
+ * (lpk_scene_tx_desc still works; nothing that launches work does). */
+lpk_status lpk_scene_prepare(lpk_ctx *ctx, const lpk_scene_cfg *cfg, lpk_scene **out);
+void lpk_scene_free(lpk_scene *s);
+int32_t lpk_scene_n_work(const lpk_scene *s);
+lpk_status lpk_scene_work(const lpk_scene *s, int32_t work_idx, int32_t *r_idx, int32_t *b_idx);
+int64_t lpk_scene_band_samples(const lpk_scene *s, int32_t r_idx, int32_t b_idx);
+/* Active (in-band) transmitter indices of a band; returns the count. */
+int32_t lpk_scene_band_active(const lpk_scene *s, int32_t r_idx, int32_t b_idx, int32_t *active,
+                              int32_t cap);
+/* Copy transmitter tx's uploaded descriptor (tables stay owned by s). */
+lpk_status lpk_scene_tx_desc(const lpk_scene *s, int32_t tx, lpk_tx_desc *out);
+/* Fill the band descriptor generate_band would use for (r_idx, b_idx). */
+lpk_status lpk_scene_band_desc(const lpk_scene *s, int32_t r_idx, int32_t b_idx, uint64_t seed_base,
+                               int32_t work_idx, lpk_band_desc *out);
+
+/* Sink: called with each finished chunk, in order, on the calling thread.
+ * Return 0 to continue, 1 to stop after this chunk (ControlFlow::Break,
+ * src/pipeline.rs:984-989), negative to abort with LPK_EINVAL. */
+typedef int32_t (*lpk_sink_fn)(void *user, const lpk_cf32 *chunk, int64_t n);
+
+typedef struct lpk_band_result {
+    int64_t n_samples;          /* samples handed to the sink */
+    int32_t stopped_early;
+    int32_t n_active;
+    uint8_t unoccluded[256];    /* per active transmitter (pipeline.rs:905) */
+} lpk_band_result;
+
+enum { LPK_NOISE_OFF = 0, LPK_NOISE_ON = 1 };
+
+/* generate_band (src/pipeline.rs:836-1019) on the GPU: the chunk loop with
+ * the receiver's clock stream (host walk, or deterministic on the device
+ * when the clock has no random part), the band-overlap gate, the fan-out
+ * kernel, AWGN and the rx chain, handing each chunk to `sink`.
+ * `noise` = LPK_NOISE_OFF skips AWGN (deterministic comparisons). */
+lpk_status lpk_generate_band(lpk_scene *s, int32_t r_idx, int32_t b_idx, uint64_t seed_base,
+                             int32_t work_idx, int64_t chunk_samples, int32_t noise,
+                             lpk_sink_fn sink, void *user, lpk_band_result *result);
+
+/* Stream one band to <dir>/<name>.iq.c64 (raw little-endian complex64,
+ * StreamingC64Writer, src/output/mod.rs:100-147). The JSON sidecar is
+ * written by the caller, which holds the descriptor. */
+lpk_status lpk_generate_band_to_file(lpk_scene *s, int32_t r_idx, int32_t b_idx, uint64_t seed_base,
+                                     int32_t work_idx, int64_t chunk_samples, int32_t noise,
+                                     const char *path, lpk_band_result *result);
+
+/* Host clock stream (ClockStream, src/clock/mod.rs:229-347) exposed for
+ * tests: delta_t_at over n monotone times. */
+typedef struct lpk_clock lpk_clock;
+lpk_status lpk_clock_new(const lpk_clock_cfg *spec, double start_epoch, double master_rate_hz,
+                         uint64_t seed, lpk_clock **out);
+lpk_status lpk_clock_delta_t(lpk_clock *c, const double *t, int64_t n, double *out);
+void lpk_clock_free(lpk_clock *c);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LIPIKA_CUDA_H */

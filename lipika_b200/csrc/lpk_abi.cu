@@ -1,0 +1,505 @@
+// lpk_abi.cu — context, transmitter upload and the kernel-level C ABI
+// (include/lipika_cuda.h).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "lpk_internal.h"
+
+using lpk::DevBand;
+using lpk::DevTx;
+
+namespace {
+std::mutex g_err_mu;
+std::string g_err;
+}  // namespace
+
+namespace lpk {
+
+lpk_status fail(lpk_ctx *ctx, lpk_status code, const std::string &msg) {
+    if (ctx) ctx->err = msg;
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_err = msg;
+    return code;
+}
+
+lpk_status cuda_fail(lpk_ctx *ctx, cudaError_t e, const char *what) {
+    char buf[512];
+    snprintf(buf, sizeof buf, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+    return fail(ctx, LPK_ECUDA, buf);
+}
+
+lpk_status ensure_scratch(lpk_ctx *ctx, size_t bytes) {
+    if (bytes <= ctx->scratch_bytes) return LPK_OK;
+    if (ctx->d_scratch) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->d_scratch);
+        ctx->d_scratch = nullptr;
+        ctx->scratch_bytes = 0;
+    }
+    size_t want = bytes + bytes / 4;
+    cudaError_t e = cudaMalloc(&ctx->d_scratch, want);
+    if (e != cudaSuccess) {
+        ctx->d_scratch = nullptr;
+        return fail(ctx, LPK_ENOMEM, std::string("device scratch allocation failed: ") + cudaGetErrorString(e));
+    }
+    ctx->scratch_bytes = want;
+    return LPK_OK;
+}
+
+lpk_status ensure_pinned(lpk_ctx *ctx, size_t bytes) {
+    if (bytes <= ctx->pinned_bytes) return LPK_OK;
+    if (ctx->h_pinned) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFreeHost(ctx->h_pinned);
+        ctx->h_pinned = nullptr;
+        ctx->pinned_bytes = 0;
+    }
+    size_t want = bytes + bytes / 4;
+    cudaError_t e = cudaMallocHost(&ctx->h_pinned, want);
+    if (e != cudaSuccess) {
+        ctx->h_pinned = nullptr;
+        return fail(ctx, LPK_ENOMEM, std::string("pinned staging allocation failed: ") + cudaGetErrorString(e));
+    }
+    ctx->pinned_bytes = want;
+    return LPK_OK;
+}
+
+static bool finite(double x) { return std::isfinite(x); }
+
+// Lower an lpk_band_desc to the device constants, computing once what the
+// reference computes once per band (generate_band, pipeline.rs:853-895;
+// RxChain::from_config and PostOp parameters, rx/mod.rs:83-137).
+lpk_status build_dev_band(lpk_ctx *ctx, const lpk_band_desc *d, int64_t i0, int64_t n, DevBand &b) {
+    memset(&b, 0, sizeof b);
+    if (!d) return fail(ctx, LPK_EINVAL, "band descriptor is NULL");
+    if (!(d->fs_hz > 0.0) || !finite(d->fs_hz)) return fail(ctx, LPK_EINVAL, "band fs_hz must be positive and finite");
+    if (!finite(d->lo_hz) || !finite(d->epoch_unix)) return fail(ctx, LPK_EINVAL, "band lo_hz/epoch must be finite");
+    if (!(d->noise_power_w >= 0.0) && !(d->noise_power_w < 0.0))
+        return fail(ctx, LPK_EINVAL, "band noise_power_w is NaN");
+    if (n < 0 || i0 < 0) return fail(ctx, LPK_EINVAL, "chunk start and length must be non-negative");
+    if (d->rx_kind != LPK_RX_STATIONARY && d->rx_kind != LPK_RX_PER_SAMPLE)
+        return fail(ctx, LPK_EINVAL, "unknown rx_kind");
+    if (d->clock_mode != LPK_CLOCK_HOST && d->clock_mode != LPK_CLOCK_DETERMINISTIC)
+        return fail(ctx, LPK_EINVAL, "clock_mode not supported by this entry point");
+    if (d->n_post < 0 || d->n_post > 3) return fail(ctx, LPK_EINVAL, "n_post must be 0..3");
+    b.epoch = d->epoch_unix;
+    b.fs = d->fs_hz;
+    b.lo = d->lo_hz;
+    b.inv_c = 1.0 / kSpeedOfLight;
+    b.i0 = i0;
+    b.n = n;
+    b.rx_kind = d->rx_kind;
+    b.clock_mode = d->clock_mode;
+    for (int k = 0; k < 3; ++k) b.rx[k] = d->rx_ecef[k];
+    b.clock_offset = d->clock_offset_s;
+    b.clock_y0 = d->clock_y0;
+    if (d->noise_power_w > 0.0) {
+        b.has_noise = 1;
+        b.noise_std = (float)std::sqrt(d->noise_power_w / 2.0);  // channel/mod.rs:328
+        b.noise_seed = d->noise_seed;
+    }
+    b.has_antenna = d->has_antenna;
+    b.has_cutoff = d->has_cutoff;
+    b.ant_peak = d->ant_peak_dbi;
+    b.ant_horizon = d->ant_horizon_dbi;
+    b.ant_fb = d->ant_fb_db;
+    b.ant_cutoff = d->ant_cutoff_deg;
+    b.n_post = d->n_post;
+    for (int k = 0; k < d->n_post; ++k) {
+        const lpk_post_op &op = d->post[k];
+        b.post_kind[k] = op.kind;
+        if (op.kind == LPK_POST_GAIN) {
+            b.post_a[k] = powf(10.0f, (float)(op.param / 20.0));
+        } else if (op.kind == LPK_POST_NONLINEARITY) {
+            if (!(op.param > 0.0)) return fail(ctx, LPK_EINVAL, "nonlinearity iip3_w must be positive");
+            b.post_a[k] = (float)(4.0 / 3.0 / op.param);
+        } else if (op.kind == LPK_POST_ADC) {
+            uint32_t bits = op.bits < 2 ? 2 : op.bits;
+            if (bits > 63) return fail(ctx, LPK_EINVAL, "adc bits must be at most 63");
+            float fs = (float)op.param;
+            float levels = (float)((1ULL << (bits - 1)) - 1ULL);
+            b.post_a[k] = fs;
+            b.post_b[k] = fs / levels;
+        } else {
+            return fail(ctx, LPK_EINVAL, "unknown post op kind");
+        }
+    }
+    return LPK_OK;
+}
+
+lpk_status check_active(lpk_ctx *ctx, const int32_t *active, int32_t n_active) {
+    if (n_active < 0 || n_active > 256) return fail(ctx, LPK_EINVAL, "n_active must be 0..256");
+    if (n_active > 0 && !active) return fail(ctx, LPK_EINVAL, "active_tx is NULL");
+    for (int32_t k = 0; k < n_active; ++k)
+        if (active[k] < 0 || active[k] >= ctx->n_tx)
+            return fail(ctx, LPK_EINVAL, "active_tx index out of range of the uploaded scene");
+    return LPK_OK;
+}
+
+}  // namespace lpk
+
+using namespace lpk;
+
+extern "C" {
+
+const char *lpk_version(void) { return "lipika_b200 0.1 (sm_100a)"; }
+
+const char *lpk_global_last_error(void) {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    static thread_local std::string copy;
+    copy = g_err;
+    return copy.c_str();
+}
+
+const char *lpk_last_error(const lpk_ctx *ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+lpk_status lpk_ctx_create(lpk_ctx **out, int32_t device) {
+    if (!out) return fail(nullptr, LPK_EINVAL, "out is NULL");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaGetDeviceCount");
+    if (device < 0 || device >= count) return fail(nullptr, LPK_EINVAL, "device index out of range");
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaSetDevice");
+    lpk_ctx *c = new (std::nothrow) lpk_ctx();
+    if (!c) return fail(nullptr, LPK_ENOMEM, "context allocation failed");
+    c->device = device;
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev_start);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev_stop);
+    if (e != cudaSuccess) {
+        lpk_status st = cuda_fail(nullptr, e, "stream/event creation");
+        lpk_ctx_destroy(c);
+        return st;
+    }
+    *out = c;
+    return LPK_OK;
+}
+
+static void free_scene(lpk_ctx *c) {
+    for (void *p : c->scene_allocs) cudaFree(p);
+    c->scene_allocs.clear();
+    c->h_tx.clear();
+    c->d_tx = nullptr;
+    c->n_tx = 0;
+}
+
+void lpk_ctx_destroy(lpk_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_scene(c);
+    if (c->d_scratch) cudaFree(c->d_scratch);
+    if (c->h_pinned) cudaFreeHost(c->h_pinned);
+    if (c->ev_start) cudaEventDestroy(c->ev_start);
+    if (c->ev_stop) cudaEventDestroy(c->ev_stop);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+static lpk_status upload_bytes(lpk_ctx *c, const void *src, size_t bytes, void **dst) {
+    *dst = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(dst, bytes);
+    if (e != cudaSuccess) return fail(c, LPK_ENOMEM, std::string("scene allocation failed: ") + cudaGetErrorString(e));
+    c->scene_allocs.push_back(*dst);
+    if (src) {
+        e = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_fail(c, e, "scene upload");
+    } else {
+        cudaMemset(*dst, 0, bytes);
+    }
+    return LPK_OK;
+}
+
+lpk_status lpk_scene_upload(lpk_ctx *c, const lpk_tx_desc *tx, int32_t n_tx) {
+    if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
+    if (n_tx < 0 || (n_tx > 0 && !tx)) return fail(c, LPK_EINVAL, "bad transmitter array");
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    free_scene(c);
+    std::vector<DevTx> h((size_t)n_tx);
+    for (int32_t i = 0; i < n_tx; ++i) {
+        const lpk_tx_desc &s = tx[i];
+        DevTx &d = h[i];
+        memset(&d, 0, sizeof d);
+        if (!(s.carrier_hz > 0.0) || !std::isfinite(s.carrier_hz))
+            return fail(c, LPK_EINVAL, "transmitter carrier_hz must be positive and finite");
+        if (!(s.tx_power_w >= 0.0) || !std::isfinite(s.tx_power_w))
+            return fail(c, LPK_EINVAL, "transmitter tx_power_w must be finite and non-negative");
+        d.traj_kind = s.traj_kind;
+        d.sig_kind = s.sig_kind;
+        d.nav_kind = s.nav_kind;
+        d.has_repeat = s.has_repeat;
+        d.sx = s.stationary_ecef[0];
+        d.sy = s.stationary_ecef[1];
+        d.sz = s.stationary_ecef[2];
+        if (s.traj_kind == LPK_TX_TRAJ_PRECOMPUTED) {
+            if (s.grid_n < 2 || !s.grid_xyz || !(s.grid_dt_s > 0.0))
+                return fail(c, LPK_EINVAL, "precomputed trajectory needs >= 2 grid points and dt > 0");
+            std::vector<double4> g((size_t)s.grid_n);
+            for (int64_t k = 0; k < s.grid_n; ++k)
+                g[k] = make_double4(s.grid_xyz[k], s.grid_xyz[s.grid_n + k], s.grid_xyz[2 * s.grid_n + k], 0.0);
+            void *p;
+            lpk_status st = upload_bytes(c, g.data(), sizeof(double4) * g.size(), &p);
+            if (st) return st;
+            d.grid = (const double4 *)p;
+            d.grid_n = s.grid_n;
+            d.t0 = s.grid_t0_unix;
+            d.dt = s.grid_dt_s;
+            d.inv_dt = 1.0 / s.grid_dt_s;
+        } else if (s.traj_kind != LPK_TX_TRAJ_STATIONARY) {
+            return fail(c, LPK_EINVAL, "unknown trajectory kind");
+        }
+        d.carrier = s.carrier_hz;
+        d.neg_tau_src = -kTau * s.carrier_hz;                              // channel/mod.rs:239
+        double wavelength = kSpeedOfLight / s.carrier_hz;                 // :209
+        d.amp_factor = (wavelength / (2.0 * kTau)) * std::sqrt(s.tx_power_w);  // :210, :243
+        d.epoch_rel = s.epoch_rel_s;
+        d.rate = s.rate_hz;
+        d.repeat_from = s.repeat_from;
+        d.n_sym = s.n_sym;
+        void *p = nullptr;
+        lpk_status st = LPK_OK;
+        switch (s.sig_kind) {
+        case LPK_SIG_CW:
+            d.cw_omega = kTau * s.cw_offset_hz;  // cw.rs:43
+            d.cw_phase0 = s.cw_phase0;
+            d.cw_anchored = s.cw_anchored;
+            break;
+        case LPK_SIG_BPSK:
+            if (s.n_sym < 0 || (s.n_sym > 0 && !s.pm_bits)) return fail(c, LPK_EINVAL, "bpsk table missing");
+            st = upload_bytes(c, s.pm_bits, (size_t)s.n_sym, &p);
+            d.pm = (const int8_t *)p;
+            break;
+        case LPK_SIG_OOK:
+            if (s.n_sym < 0 || (s.n_sym > 0 && !s.ook_bits)) return fail(c, LPK_EINVAL, "ook table missing");
+            st = upload_bytes(c, s.ook_bits, (size_t)s.n_sym, &p);
+            d.ook = (const uint8_t *)p;
+            break;
+        case LPK_SIG_QAM16:
+            if (s.n_sym < 0 || (s.n_sym > 0 && !s.symbols)) return fail(c, LPK_EINVAL, "qam16 table missing");
+            st = upload_bytes(c, s.symbols, sizeof(float2) * (size_t)s.n_sym, &p);
+            d.sym = (const float2 *)p;
+            break;
+        case LPK_SIG_CA_CODE:
+            if (!s.chips) return fail(c, LPK_EINVAL, "ca_code chip table missing");
+            for (int k = 0; k < 1023; ++k) {
+                if (s.chips[k] != 1 && s.chips[k] != -1) return fail(c, LPK_EINVAL, "ca_code chips must be ±1");
+                if (s.chips[k] < 0) d.chip_neg[k >> 5] |= 1u << (k & 31);
+            }
+            d.nav_seed = s.nav_seed;
+            if (s.nav_kind == LPK_NAV_FULL) {
+                if (s.nav_n < 0 || (s.nav_n > 0 && !s.nav_bits)) return fail(c, LPK_EINVAL, "nav table missing");
+                st = upload_bytes(c, s.nav_bits, (size_t)s.nav_n, &p);
+                d.nav_bits = (const int8_t *)p;
+                d.nav_n = s.nav_n;
+            } else if (s.nav_kind != LPK_NAV_OFF && s.nav_kind != LPK_NAV_DUMMY) {
+                return fail(c, LPK_EINVAL, "unknown nav kind");
+            }
+            break;
+        default:
+            return fail(c, LPK_EINVAL, "unknown signal kind");
+        }
+        if (st) return st;
+        if ((s.sig_kind == LPK_SIG_BPSK || s.sig_kind == LPK_SIG_OOK || s.sig_kind == LPK_SIG_QAM16) &&
+            !(s.rate_hz > 0.0))
+            return fail(c, LPK_EINVAL, "symbol rate must be positive");
+        if (s.has_gate) {
+            if (!(s.gate_period_s > 0.0) || !std::isfinite(s.gate_period_s) || s.gate_n < 0 ||
+                (s.gate_n > 0 && !s.gate_on))
+                return fail(c, LPK_EINVAL, "bad burst gate");
+            d.has_gate = 1;
+            d.gate_n = s.gate_n;
+            d.gate_period = s.gate_period_s;
+            d.gate_phase = s.gate_phase_s;
+            st = upload_bytes(c, s.gate_on, sizeof(double2) * (size_t)s.gate_n, &p);
+            if (st) return st;
+            d.gate_on = (const double2 *)p;
+        }
+    }
+    void *p;
+    lpk_status st = upload_bytes(c, h.data(), sizeof(DevTx) * h.size(), &p);
+    if (st) return st;
+    c->d_tx = (DevTx *)p;
+    c->h_tx = std::move(h);
+    c->n_tx = n_tx;
+    return LPK_OK;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+lpk_status lpk_band_chunk_device(lpk_ctx *c, const lpk_band_desc *band, const int32_t *active,
+                                 int32_t n_active, int64_t i0, int64_t n, const double *d_delta,
+                                 const double *d_rxpos, lpk_cf32 *d_out, uint8_t *d_unocc) {
+    if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
+    DevBand b;
+    lpk_status st = build_dev_band(c, band, i0, n, b);
+    if (st) return st;
+    if ((st = check_active(c, active, n_active))) return st;
+    if (b.clock_mode == LPK_CLOCK_HOST && n > 0 && !d_delta) return fail(c, LPK_EINVAL, "delta_t is NULL");
+    if (b.rx_kind == LPK_RX_PER_SAMPLE && n > 0 && !d_rxpos) return fail(c, LPK_EINVAL, "rx_pos3n is NULL");
+    if (n > 0 && !d_out) return fail(c, LPK_EINVAL, "out is NULL");
+    b.delta = d_delta;
+    b.rxpos = d_rxpos;
+    cudaSetDevice(c->device);
+    // active list and unoccluded words live in the small head of the scratch
+    size_t head = align256(sizeof(int32_t) * 256) + align256(sizeof(uint32_t) * 256);
+    if ((st = ensure_scratch(c, head))) return st;
+    int32_t *d_active = (int32_t *)c->d_scratch;
+    uint32_t *d_uw = (uint32_t *)((char *)c->d_scratch + align256(sizeof(int32_t) * 256));
+    cudaError_t e = cudaMemcpyAsync(d_active, active, sizeof(int32_t) * (size_t)n_active, cudaMemcpyHostToDevice,
+                                    c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_uw, 0, sizeof(uint32_t) * 256, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "chunk setup");
+    e = launch_band_reference(b, c->d_tx, d_active, n_active, (float2 *)d_out, d_uw, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "fan-out kernel launch");
+    (void)d_unocc;
+    return LPK_OK;
+}
+
+lpk_status lpk_sync(lpk_ctx *c) {
+    if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "stream synchronize");
+    return LPK_OK;
+}
+
+lpk_status lpk_band_chunk(lpk_ctx *c, const lpk_band_desc *band, const int32_t *active, int32_t n_active,
+                          int64_t i0, int64_t n, const double *delta_t, const double *rx_pos3n, lpk_cf32 *out,
+                          uint8_t *unoccluded) {
+    if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
+    DevBand b;
+    lpk_status st = build_dev_band(c, band, i0, n, b);
+    if (st) return st;
+    if ((st = check_active(c, active, n_active))) return st;
+    if (b.clock_mode == LPK_CLOCK_HOST && n > 0 && !delta_t) return fail(c, LPK_EINVAL, "delta_t is NULL");
+    if (b.rx_kind == LPK_RX_PER_SAMPLE && n > 0 && !rx_pos3n) return fail(c, LPK_EINVAL, "rx_pos3n is NULL");
+    if (n > 0 && !out) return fail(c, LPK_EINVAL, "out is NULL");
+    cudaSetDevice(c->device);
+    size_t off_active = 0;
+    size_t off_uw = align256(sizeof(int32_t) * 256);
+    size_t off_delta = off_uw + align256(sizeof(uint32_t) * 256);
+    size_t n_delta = b.clock_mode == LPK_CLOCK_HOST ? (size_t)n : 0;
+    size_t off_rx = off_delta + align256(sizeof(double) * n_delta);
+    size_t n_rx = b.rx_kind == LPK_RX_PER_SAMPLE ? 3 * (size_t)n : 0;
+    size_t off_out = off_rx + align256(sizeof(double) * n_rx);
+    size_t total = off_out + align256(sizeof(float2) * (size_t)n);
+    if ((st = ensure_scratch(c, total))) return st;
+    char *base = (char *)c->d_scratch;
+    int32_t *d_active = (int32_t *)(base + off_active);
+    uint32_t *d_uw = (uint32_t *)(base + off_uw);
+    double *d_delta = (double *)(base + off_delta);
+    double *d_rx = (double *)(base + off_rx);
+    float2 *d_out = (float2 *)(base + off_out);
+    cudaError_t e = cudaMemcpyAsync(d_active, active, sizeof(int32_t) * (size_t)n_active, cudaMemcpyHostToDevice,
+                                    c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_uw, 0, sizeof(uint32_t) * 256, c->stream);
+    if (e == cudaSuccess && n_delta)
+        e = cudaMemcpyAsync(d_delta, delta_t, sizeof(double) * n_delta, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && n_rx)
+        e = cudaMemcpyAsync(d_rx, rx_pos3n, sizeof(double) * n_rx, cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "chunk upload");
+    b.delta = d_delta;
+    b.rxpos = d_rx;
+    e = launch_band_reference(b, c->d_tx, d_active, n_active, d_out, d_uw, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "fan-out kernel launch");
+    if (n > 0) e = cudaMemcpyAsync(out, d_out, sizeof(float2) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
+    uint32_t uw[256];
+    if (e == cudaSuccess && unoccluded && n_active > 0)
+        e = cudaMemcpyAsync(uw, d_uw, sizeof(uint32_t) * (size_t)n_active, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "fan-out kernel");
+    if (unoccluded)
+        for (int32_t k = 0; k < n_active; ++k)
+            unoccluded[k] |= (uint8_t)(b.has_antenna ? (uw[k] != 0) : (n > 0));
+    return LPK_OK;
+}
+
+lpk_status lpk_solve_emission_times(lpk_ctx *c, int32_t tx, const double *obs3n, const double *t_rel_utc,
+                                    int64_t n, double epoch, int32_t iterations, double *t_emit,
+                                    double *ranges) {
+    if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
+    if (tx < 0 || tx >= c->n_tx) return fail(c, LPK_EINVAL, "transmitter index out of range");
+    if (n < 0 || iterations < 0 || iterations > 64) return fail(c, LPK_EINVAL, "bad n or iterations");
+    if (n == 0) return LPK_OK;
+    if (!obs3n || !t_rel_utc || !t_emit || !ranges) return fail(c, LPK_EINVAL, "NULL array");
+    cudaSetDevice(c->device);
+    size_t bytes = sizeof(double) * (size_t)n;
+    lpk_status st = ensure_scratch(c, 6 * bytes + 1024);
+    if (st) return st;
+    double *d_obs = (double *)c->d_scratch, *d_t = d_obs + 3 * n, *d_te = d_t + n, *d_r = d_te + n;
+    cudaError_t e = cudaMemcpyAsync(d_obs, obs3n, 3 * bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_t, t_rel_utc, bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = launch_solve(c->d_tx, tx, d_obs, d_t, n, epoch, iterations, 1.0 / kSpeedOfLight, d_te, d_r, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(t_emit, d_te, bytes, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ranges, d_r, bytes, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "emission solve");
+    return LPK_OK;
+}
+
+lpk_status lpk_tx_contribution(lpk_ctx *c, const lpk_band_desc *band, int32_t tx, int64_t i0, int64_t n,
+                               const double *delta_t, const double *rx_pos3n, lpk_cf32 *out, double *phase_out,
+                               double *t_emit_out, double *range_out) {
+    if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
+    if (tx < 0 || tx >= c->n_tx) return fail(c, LPK_EINVAL, "transmitter index out of range");
+    DevBand b;
+    lpk_status st = build_dev_band(c, band, i0, n, b);
+    if (st) return st;
+    if (b.clock_mode == LPK_CLOCK_HOST && n > 0 && !delta_t) return fail(c, LPK_EINVAL, "delta_t is NULL");
+    if (b.rx_kind == LPK_RX_PER_SAMPLE && n > 0 && !rx_pos3n) return fail(c, LPK_EINVAL, "rx_pos3n is NULL");
+    if (n == 0) return LPK_OK;
+    if (!out) return fail(c, LPK_EINVAL, "out is NULL");
+    cudaSetDevice(c->device);
+    size_t bytes = sizeof(double) * (size_t)n;
+    lpk_status s2 = ensure_scratch(c, 8 * bytes + 4096);
+    if (s2) return s2;
+    double *d_delta = (double *)c->d_scratch;
+    double *d_rx = d_delta + n;
+    double *d_phase = d_rx + 3 * n;
+    double *d_te = d_phase + n;
+    double *d_r = d_te + n;
+    float2 *d_out = (float2 *)(d_r + n);
+    cudaError_t e = cudaSuccess;
+    if (b.clock_mode == LPK_CLOCK_HOST) e = cudaMemcpyAsync(d_delta, delta_t, bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && b.rx_kind == LPK_RX_PER_SAMPLE)
+        e = cudaMemcpyAsync(d_rx, rx_pos3n, 3 * bytes, cudaMemcpyHostToDevice, c->stream);
+    b.delta = d_delta;
+    b.rxpos = d_rx;
+    if (e == cudaSuccess) e = launch_tx_contribution(b, c->d_tx, tx, d_out, d_phase, d_te, d_r, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, sizeof(float2) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && phase_out) e = cudaMemcpyAsync(phase_out, d_phase, bytes, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && t_emit_out) e = cudaMemcpyAsync(t_emit_out, d_te, bytes, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && range_out) e = cudaMemcpyAsync(range_out, d_r, bytes, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "transmitter contribution");
+    return LPK_OK;
+}
+
+lpk_status lpk_rx_chain_apply(lpk_ctx *c, const lpk_band_desc *band, lpk_cf32 *iq, int64_t n) {
+    if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
+    lpk_band_desc d = band ? *band : lpk_band_desc{};
+    d.noise_power_w = 0.0;
+    d.clock_mode = LPK_CLOCK_DETERMINISTIC;
+    DevBand b;
+    lpk_status st = build_dev_band(c, band ? &d : nullptr, 0, n, b);
+    if (st) return st;
+    if (n == 0) return LPK_OK;
+    if (!iq) return fail(c, LPK_EINVAL, "iq is NULL");
+    cudaSetDevice(c->device);
+    if ((st = ensure_scratch(c, sizeof(float2) * (size_t)n))) return st;
+    float2 *d_iq = (float2 *)c->d_scratch;
+    cudaError_t e = cudaMemcpyAsync(d_iq, iq, sizeof(float2) * (size_t)n, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = launch_rx_chain(b, d_iq, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(iq, d_iq, sizeof(float2) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "rx chain");
+    return LPK_OK;
+}
+
+}  // extern "C"

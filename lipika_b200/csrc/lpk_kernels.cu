@@ -1,0 +1,188 @@
+// lpk_kernels.cu — the fan-out kernels.
+//
+// k_band_reference: one thread per band sample, the band's in-band
+// transmitters in fixed order, each evaluated with the reference's exact
+// f64 operation sequence (emission solve, s(t), mix), summed in f32 in
+// transmitter order, then AWGN and the rx chain. This is the all-FP64 path
+// that replaces src/pipeline.rs:943-983 bit-for-bit (up to the last ulp of
+// CUDA's sin/cos).
+#include "lpk_internal.h"
+
+namespace lpk {
+
+namespace {
+
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ double band_delta(const DevBand &b, int64_t j, double t_local) {
+    if (b.clock_mode == LPK_CLOCK_DETERMINISTIC)  // (ε=0 + flicker=0) + c + m·t, clock/mod.rs:311-345
+        return __dadd_rn(0.0, __dadd_rn(b.clock_offset, __dmul_rn(b.clock_y0, t_local)));
+    return b.delta[j];
+}
+
+__device__ __forceinline__ void band_rx(const DevBand &b, int64_t j, double &ox, double &oy, double &oz) {
+    if (b.rx_kind == LPK_RX_STATIONARY) { ox = b.rx[0]; oy = b.rx[1]; oz = b.rx[2]; return; }
+    ox = b.rxpos[j];
+    oy = b.rxpos[b.n + j];
+    oz = b.rxpos[2 * b.n + j];
+}
+
+// One transmitter's contribution at one sample (channel/mod.rs:251-267).
+// Returns false when the antenna gain is zero (the sample is skipped and
+// the per-transmitter buffer keeps its +0).
+__device__ __forceinline__ bool contribution(const DevTx &tx, const DevBand &b, double t_local, double tu,
+                                             double delta, double ox, double oy, double oz, float &cr,
+                                             float &ci, double *phase_out, double *temit_out,
+                                             double *range_out) {
+    double t_emit, r;
+    solve_reference(tx, tu, ox, oy, oz, b.epoch, 2, b.inv_c, t_emit, r);  // NEWTON_ITERATIONS
+    if (temit_out) *temit_out = t_emit;
+    if (range_out) *range_out = r;
+    float2 bb = baseband(tx, t_emit);
+    float g = 1.0f;
+    if (b.has_antenna) {
+        g = antenna_gain(tx, b, __dadd_rn(b.epoch, t_emit), ox, oy, oz);
+        if (g == 0.0f) {
+            if (phase_out) *phase_out = 0.0;
+            return false;
+        }
+    }
+    double delay = __dmul_rn(r, b.inv_c);
+    double tau_if = __dmul_rn(kTau, __dsub_rn(tx.carrier, b.lo));
+    double phase = __dadd_rn(__dmul_rn(tx.neg_tau_src, __dadd_rn(delay, delta)), __dmul_rn(tau_if, t_local));
+    if (phase_out) *phase_out = remainder(phase, kTau);
+    double sp, cp;
+    sincos(phase, &sp, &cp);
+    float amp = __fmul_rn((float)__ddiv_rn(tx.amp_factor, r), g);
+    float cpf = (float)cp, spf = (float)sp;
+    cr = __fadd_rn(0.0f, __fmul_rn(amp, __fsub_rn(__fmul_rn(bb.x, cpf), __fmul_rn(bb.y, spf))));
+    ci = __fadd_rn(0.0f, __fmul_rn(amp, __fadd_rn(__fmul_rn(bb.x, spf), __fmul_rn(bb.y, cpf))));
+    return true;
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_band_reference(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__restrict__ active,
+                 int32_t n_active, float2 *__restrict__ out, uint32_t *__restrict__ unocc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    DevTx *stx = reinterpret_cast<DevTx *>(smem_raw);
+    {
+        const int words = (int)(sizeof(DevTx) / 8);
+        for (int k = 0; k < n_active; ++k) {
+            const uint64_t *src = reinterpret_cast<const uint64_t *>(txs + active[k]);
+            uint64_t *dst = reinterpret_cast<uint64_t *>(stx + k);
+            for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = src[w];
+        }
+    }
+    __syncthreads();
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = j < b.n;
+    const int64_t g = b.i0 + j;
+    double t_local = 0.0, delta = 0.0, tu = 0.0, ox = 0.0, oy = 0.0, oz = 0.0;
+    if (live) {
+        t_local = __ddiv_rn((double)g, b.fs);  // src/pipeline.rs:918
+        delta = band_delta(b, j, t_local);
+        tu = __dsub_rn(t_local, delta);         // :927
+        band_rx(b, j, ox, oy, oz);
+    }
+    float acc_re = 0.0f, acc_im = 0.0f;
+    for (int k = 0; k < n_active; ++k) {
+        float cr = 0.0f, ci = 0.0f;
+        bool on = false;
+        if (live) {
+            on = contribution(stx[k], b, t_local, tu, delta, ox, oy, oz, cr, ci, nullptr, nullptr, nullptr);
+            if (on) {  // fixed-order Σ, pipeline.rs:966-977
+                acc_re = __fadd_rn(acc_re, cr);
+                acc_im = __fadd_rn(acc_im, ci);
+            }
+        }
+        if (b.has_antenna && unocc) {
+            unsigned any = __ballot_sync(0xffffffffu, on);
+            if ((threadIdx.x & 31) == 0 && any) atomicOr(unocc + k, 1u);
+        }
+    }
+    if (!live) return;
+    out[j] = band_epilogue(b, acc_re, acc_im, g);
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_tx_contribution(const DevBand b, const DevTx *__restrict__ txs, int32_t tx_idx, float2 *__restrict__ out,
+                  double *phase, double *temit, double *range) {
+    __shared__ DevTx stx;
+    if (threadIdx.x == 0) stx = txs[tx_idx];
+    __syncthreads();
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= b.n) return;
+    const int64_t g = b.i0 + j;
+    double t_local = __ddiv_rn((double)g, b.fs);
+    double delta = band_delta(b, j, t_local);
+    double tu = __dsub_rn(t_local, delta);
+    double ox, oy, oz;
+    band_rx(b, j, ox, oy, oz);
+    float cr = 0.0f, ci = 0.0f;
+    contribution(stx, b, t_local, tu, delta, ox, oy, oz, cr, ci, phase ? phase + j : nullptr,
+                 temit ? temit + j : nullptr, range ? range + j : nullptr);
+    out[j] = make_float2(cr, ci);
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_solve(const DevTx *__restrict__ txs, int32_t tx_idx, const double *__restrict__ obs,
+        const double *__restrict__ t, int64_t n, double epoch, int32_t iterations, double inv_c,
+        double *__restrict__ temit, double *__restrict__ range) {
+    __shared__ DevTx stx;
+    if (threadIdx.x == 0) stx = txs[tx_idx];
+    __syncthreads();
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double te, r;
+    solve_reference(stx, t[j], obs[j], obs[n + j], obs[2 * n + j], epoch, iterations, inv_c, te, r);
+    temit[j] = te;
+    range[j] = r;
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_rx_chain(const DevBand b, float2 *__restrict__ iq) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= b.n) return;
+    float2 v = iq[j];
+    iq[j] = band_epilogue(b, v.x, v.y, b.i0 + j);
+}
+
+inline unsigned grid_for(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
+
+}  // namespace
+
+cudaError_t launch_band_reference(const DevBand &b, const DevTx *d_tx, const int32_t *d_active,
+                                  int32_t n_active, float2 *d_out, uint32_t *d_unocc, cudaStream_t s) {
+    if (b.n <= 0) return cudaSuccess;
+    size_t smem = sizeof(DevTx) * (size_t)n_active;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_band_reference, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    k_band_reference<<<grid_for(b.n), kBlock, smem, s>>>(b, d_tx, d_active, n_active, d_out, d_unocc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tx_contribution(const DevBand &b, const DevTx *d_tx, int32_t tx, float2 *d_out,
+                                   double *d_phase, double *d_temit, double *d_range, cudaStream_t s) {
+    if (b.n <= 0) return cudaSuccess;
+    k_tx_contribution<<<grid_for(b.n), kBlock, 0, s>>>(b, d_tx, tx, d_out, d_phase, d_temit, d_range);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rx_chain(const DevBand &b, float2 *d_iq, cudaStream_t s) {
+    if (b.n <= 0) return cudaSuccess;
+    k_rx_chain<<<grid_for(b.n), kBlock, 0, s>>>(b, d_iq);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_solve(const DevTx *d_tx, int32_t tx, const double *d_obs, const double *d_t, int64_t n,
+                         double epoch, int32_t iterations, double inv_c, double *d_temit, double *d_range,
+                         cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_solve<<<grid_for(n), kBlock, 0, s>>>(d_tx, tx, d_obs, d_t, n, epoch, iterations, inv_c, d_temit, d_range);
+    return cudaGetLastError();
+}
+
+}  // namespace lpk
