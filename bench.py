@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Throughput of the B200 IQ-generation backend: tx·rx IQ samples per second.
+
+Workload (one "step"): the dual-band 120 s scene — a 437 MHz BPSK LEO beacon
+(9.6 kbit/s, 287,968 payload bits) seen at 48 kS/s plus GPS C/A PRN 1-6 on
+circular 26,578 km orbits seen at 2.048 MS/s, one Glasgow receiver whose
+clock has a white-FM walk (Allan 1e-11 @1 s, y0 = 0.5e-6), thermal AWGN at
+290 K. 5.76e6 + 6 x 2.4576e8 = 1.4803e9 tx·rx samples per step. Synthetic
+scene (no dataset exists for this path); the payload is seeded.
+
+  value : the whole scene with every input resident in HBM (scene tables
+          uploaded once, clock walk and AWGN generated on the device, output
+          kept on the device), timed with CUDA events on the library's stream.
+  e2e   : the same scene through the host-level C ABI (lpk_scene_prepare +
+          lpk_generate_band) into host memory: table upload and every chunk's
+          device-to-host copy are inside the timed region.
+
+Launched plainly for 1 GPU or under torchrun for N GPUs (one replica of the
+scene per rank, weak scaling, no data-path collective). `--impl reference`
+times the CPU restatement of the reference's own loop (the oracle port; the
+Rust reference cannot be built here) on a bounded sample of the same scene.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "tx·rx IQ samples/s"
+UNIT = "tx·rx samples/s"
+WORKLOAD = ("dual_band_120s: BPSK 9.6 kbit/s LEO beacon at 437 MHz (48 kS/s band) + GPS C/A PRN 1-6 at "
+            "1575.42 MHz (2.048 MS/s band), one receiver with white-FM clock walk, AWGN at 290 K, complex64")
+FLOP_PER_SAMPLE = 76      # FP64-equivalent flops per tx·rx sample of the reference loop
+BYTES_PER_BAND_SAMPLE = 8  # complex64 written per band sample
+
+
+def _args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=30)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--duration", type=float, default=120.0, help="scene duration (s)")
+    p.add_argument("--chunk", type=int, default=1 << 24, help="samples per fan-out launch (value leg)")
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU time of the baseline sample")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def _scene(duration, seed_offset=0):
+    from tests import scenes
+    sc = scenes.config_c1(duration_s=duration)
+    return sc
+
+
+def _txrx_counts(prep):
+    total_band, total_txrx = 0, 0
+    per = []
+    for (r, b) in prep.work():
+        n = prep.n_samples(r, b)
+        k = len(prep.active(r, b))
+        per.append((r, b, n, k))
+        total_band += n
+        total_txrx += n * k
+    return per, total_band, total_txrx
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._pump, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _pump(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        time.sleep(0.05)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def _traffic_from_profile(launch_band_samples: float):
+    """DRAM bytes per launch from the committed ncu summary (scaled by band
+    samples per launch), or None."""
+    path = os.path.join(ROOT, "profiles", "fanout_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    return d["dram_bytes_per_band_sample"] * launch_band_samples
+
+
+def cpu_baseline(duration, target_s, threads=None):
+    """The oracle port (C restatement of the reference loop, per-transmitter
+    threads as rayon does) on the first S seconds of the same scene."""
+    from oracle import oracle as O
+    threads = threads or os.cpu_count() or 1
+    sc = _scene(duration)
+    osc = O.Scene(sc)
+    rate_per_s = sum(b.sample_rate_hz * len(osc.active(0, bi)) for bi, b in enumerate(sc.receivers[0].bands))
+
+    def run(seconds):
+        t0 = time.perf_counter()
+        for w, (r, b) in enumerate(osc.work()):
+            fs = sc.receivers[r].bands[b].sample_rate_hz
+            osc.generate_band(r, b, 2026, w, 1 << 20, threads, O.NOISE_SEQUENTIAL, limit=int(round(fs * seconds)))
+        return time.perf_counter() - t0
+
+    probe = 0.1
+    t = run(probe)
+    seconds = max(probe, min(duration, probe * target_s / max(t, 1e-3)))
+    t = run(seconds)
+    return {"value": seconds * rate_per_s / t, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"first {seconds:.3f} s of the {duration:.0f} s scene, both bands, AWGN on, "
+                      f"{seconds * rate_per_s:.3e} tx·rx samples in {t:.2f} s"}, seconds
+
+
+def run_reference(a):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    O.build()
+    threads = os.cpu_count() or 1
+    # each step: the same bounded sample, sized to about --cpu-seconds
+    _, sample_s = cpu_baseline(a.duration, a.cpu_seconds / max(a.steps, 1), threads)
+    from oracle import oracle as O2
+    sc = _scene(a.duration)
+    osc = O2.Scene(sc)
+    rate_per_s = sum(b.sample_rate_hz * len(osc.active(0, bi)) for bi, b in enumerate(sc.receivers[0].bands))
+    times = []
+    for it in range(a.warmup + a.steps):
+        t0 = time.perf_counter()
+        for w, (r, b) in enumerate(osc.work()):
+            fs = sc.receivers[r].bands[b].sample_rate_hz
+            osc.generate_band(r, b, 2026, w, 1 << 20, threads, O2.NOISE_SEQUENTIAL, limit=int(round(fs * sample_s)))
+        if it >= a.warmup:
+            times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = sample_s * rate_per_s * len(times) / tot
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * tot / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded scene)",
+            "config": {"workload": WORKLOAD, "duration_s": a.duration, "step": f"first {sample_s:.3f} s of the scene",
+                       "parallelism": f"{threads} host threads"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"first {sample_s:.3f} s of the scene per step (oracle port; the Rust "
+                                       "reference has no toolchain here)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(a):
+    import torch
+    from lipika_b200 import native as N
+    from lipika_b200 import pipeline as P
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    seed = 2026 + rank
+    ctx = N.Context(local)
+    L = N.lib()
+    stream = torch.cuda.ExternalStream(L.lpk_ctx_stream(ctx.h), device=torch.device("cuda", local))
+    sc = _scene(a.duration)
+    prep = P.Prepared(sc, ctx)
+    per, total_band, total_txrx = _txrx_counts(prep)
+
+    # device-resident outputs and per-band descriptors
+    bands = []
+    for w, (r, b, n, k) in enumerate(per):
+        d = prep.band_desc(r, b, seed, w)
+        if d.clock_mode == N.LPK_CLOCK_HOST:
+            d.clock_mode = N.LPK_CLOCK_DEVICE_WALK
+        act = prep.active(r, b)
+        out = torch.empty(2 * n, dtype=torch.float32, device=f"cuda:{local}")
+        bands.append((d, (C.c_int32 * max(len(act), 1))(*act), len(act), n, out))
+
+    def step():
+        for d, act, na, n, out in bands:
+            base = out.data_ptr()
+            for i0 in range(0, n, a.chunk):
+                m = min(a.chunk, n - i0)
+                N.check(L.lpk_band_chunk_device(ctx.h, C.byref(d), act, na, i0, m, None, None,
+                                                base + 8 * i0, None), ctx.h)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(a.warmup):
+        step()
+    N.check(L.lpk_sync(ctx.h), ctx.h)
+    peak_fp64 = C.c_double()
+    N.check(L.lpk_probe_fp64_peak(ctx.h, C.byref(peak_fp64)), ctx.h)
+
+    N.check(L.lpk_profile_reset(ctx.h), ctx.h)
+    N.check(L.lpk_profile_enable(ctx.h, 1), ctx.h)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    time.sleep(0.3)
+    ev0.record(stream)
+    for _ in range(a.steps):
+        step()
+    ev1.record(stream)
+    ev1.synchronize()
+    clk = clocks.stop()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    fan_ms, fan_n, all_n = C.c_double(), C.c_int64(), C.c_int64()
+    N.check(L.lpk_profile_read(ctx.h, C.byref(fan_ms), C.byref(fan_n), C.byref(all_n)), ctx.h)
+    N.check(L.lpk_profile_enable(ctx.h, 0), ctx.h)
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = total_txrx * a.steps * ws / (ms * 1e-3)
+
+    # roofline of the dominant kernel (the fan-out), from its own events
+    avg_launch_ms = fan_ms.value / max(fan_n.value, 1)
+    txrx_per_launch = total_txrx * a.steps / max(fan_n.value, 1)
+    band_per_launch = total_band * a.steps / max(fan_n.value, 1)
+    achieved_tf = FLOP_PER_SAMPLE * txrx_per_launch / (avg_launch_ms * 1e-3) / 1e12
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    hbm_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
+    traffic = _traffic_from_profile(band_per_launch)
+    achieved_gbs = BYTES_PER_BAND_SAMPLE * band_per_launch / (avg_launch_ms * 1e-3) / 1e9
+
+    # e2e through the host-level C ABI, host buffers
+    e2e = None
+    if not a.no_e2e:
+        host = np.empty(2 * max(n for _, _, n, _ in per), dtype=np.float32)
+        hptr = host.ctypes.data
+        pos = [0]
+
+        def sink(_u, ptr, n):
+            C.memmove(hptr + 8 * pos[0], ptr, 8 * n)
+            pos[0] += n
+            return 0
+
+        cb = N.SINK_FN(sink)
+        h2d = 0
+        for i in range(len(sc.transmitters)):
+            td = N.TxDesc()
+            N.check(L.lpk_scene_tx_desc(prep.h, i, C.byref(td)))
+            h2d += 24 * td.grid_n + td.n_sym * (8 if td.sig_kind == 3 else 1) + (1023 if td.sig_kind == 4 else 0)
+
+        def e2e_step():
+            p2 = P.Prepared(sc, ctx)
+            for w, (r, b) in enumerate(p2.work()):
+                pos[0] = 0
+                res = N.BandResult()
+                N.check(L.lpk_generate_band(p2.h, r, b, seed, w, P.DEFAULT_CHUNK_SAMPLES,
+                                            N.LPK_NOISE_ON | N.LPK_GEN_DEVICE_CLOCK, cb, None, C.byref(res)),
+                        ctx.h)
+            p2.close()
+
+        e2e_step()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        for _ in range(a.e2e_steps):
+            e2e_step()
+        e1.record(stream)
+        e1.synchronize()
+        wall = time.perf_counter() - t0
+        ems = max(e0.elapsed_time(e1), 1e3 * wall)
+        if dist is not None:
+            t = torch.tensor([ems], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": total_txrx * a.e2e_steps * ws / (ems * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(BYTES_PER_BAND_SAMPLE * total_band),
+               "path": "lpk_scene_prepare + lpk_generate_band (C ABI) into host memory, 2^20-sample chunks"}
+
+    base = None
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        base, _ = cpu_baseline(a.duration, a.cpu_seconds)
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded scene, no dataset)",
+        "config": {"workload": WORKLOAD, "duration_s": a.duration, "tx_rx_samples_per_step_per_gpu": total_txrx,
+                   "band_samples_per_step_per_gpu": total_band, "chunk_samples": a.chunk,
+                   "solver": "reference semantics: 2 fixed-point iterations from t-70 ms, all FP64",
+                   "clock": "white-FM walk generated on the device", "noise": "AWGN on",
+                   "parallelism": f"{ws} GPU(s), one scene replica per GPU",
+                   "l2": "output (1.97 GB/step) is larger than L2; scene tables (~3 MB) are L2-resident by design"},
+        "roofline": {"bound": "fp64", "achieved": achieved_tf, "peak": peak_fp64.value, "unit": "TFLOP/s",
+                     "frac": achieved_tf / peak_fp64.value if peak_fp64.value else None,
+                     "traffic": traffic, "kernel": "k_band_reference",
+                     "basis": f"{FLOP_PER_SAMPLE} FP64-equivalent flop per tx·rx sample x {txrx_per_launch:.4g} "
+                              f"tx·rx samples per launch / {avg_launch_ms:.3f} ms average launch (CUDA events "
+                              "on the launching stream); peak = FP64 DFMA probe measured in this run",
+                     "hbm": {"achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                             "frac": achieved_gbs / hbm_peak, "peak_source": hbm_src,
+                             "algorithmic_bytes_per_launch": BYTES_PER_BAND_SAMPLE * band_per_launch}},
+        "e2e": e2e, "gpu_launches": int(all_n.value), "clocks": clk,
+    }
+    if base is not None:
+        line["cpu_baseline"] = base
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    a = _args()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

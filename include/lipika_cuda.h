@@ -57,6 +57,23 @@ const char *lpk_last_error(const lpk_ctx *ctx);
 const char *lpk_global_last_error(void);
 /* Library version string. */
 const char *lpk_version(void);
+/* The context's CUDA stream as an opaque handle (a cudaStream_t), so a
+ * host can order its own work or timing events against the library's. */
+void *lpk_ctx_stream(lpk_ctx *ctx);
+
+/* Measurement hooks (no reference counterpart; the reference times coarse
+ * sections with profile::time, src/profile.rs:27-36). While enabled, every
+ * fan-out launch is bracketed by CUDA events on the context's stream.
+ * lpk_profile_read waits for the stream, then reports the summed fan-out
+ * kernel time, the number of fan-out launches and the number of all kernel
+ * launches since the last reset. */
+lpk_status lpk_profile_enable(lpk_ctx *ctx, int32_t on);
+lpk_status lpk_profile_reset(lpk_ctx *ctx);
+lpk_status lpk_profile_read(lpk_ctx *ctx, double *fanout_ms, int64_t *fanout_launches,
+                            int64_t *all_launches);
+/* Measured FP64 FMA throughput of the device (TFLOP/s, 2 flops per FMA)
+ * from a register-resident DFMA chain kernel timed with CUDA events. */
+lpk_status lpk_probe_fp64_peak(lpk_ctx *ctx, double *tflops);
 
 /* ------------------------------------------------------------------ */
 /* Kernel-level boundary: transmitters as already-built tables          */
@@ -183,6 +200,13 @@ lpk_status lpk_tx_contribution(lpk_ctx *ctx, const lpk_band_desc *band, int32_t 
                                lpk_cf32 *out, double *phase_out, double *t_emit_out,
                                double *range_out);
 
+/* The clock offsets Δt the fan-out uses for band samples [i0, i0 + n) under
+ * the band's clock mode (DETERMINISTIC or DEVICE_WALK), copied to host
+ * memory: ClockStream::delta_t_at (src/clock/mod.rs:329-346) evaluated on
+ * the device. */
+lpk_status lpk_clock_device_delta(lpk_ctx *ctx, const lpk_band_desc *band, int64_t i0, int64_t n,
+                                  double *delta_out);
+
 /* AWGN-free rx chain alone on n samples in place (RxChain::apply_post_sum,
  * src/rx/mod.rs:142-146): the band's post ops on caller-supplied f32 IQ,
  * so ADC codes can be compared on identical inputs. Host memory. */
@@ -224,22 +248,28 @@ typedef struct lpk_band_result {
     uint8_t unoccluded[256];    /* per active transmitter (pipeline.rs:905) */
 } lpk_band_result;
 
-enum { LPK_NOISE_OFF = 0, LPK_NOISE_ON = 1 };
+/* generate_band flags. */
+enum {
+    LPK_NOISE_OFF = 0,          /* no AWGN (deterministic comparisons) */
+    LPK_NOISE_ON = 1,           /* AWGN at the band's noise power */
+    LPK_GEN_DEVICE_CLOCK = 2    /* white-FM walk generated on the GPU (counter-based,
+                                   moment-matched) instead of the host stream */
+};
 
 /* generate_band (src/pipeline.rs:836-1019) on the GPU: the chunk loop with
- * the receiver's clock stream (host walk, or deterministic on the device
- * when the clock has no random part), the band-overlap gate, the fan-out
- * kernel, AWGN and the rx chain, handing each chunk to `sink`.
- * `noise` = LPK_NOISE_OFF skips AWGN (deterministic comparisons). */
+ * the receiver's clock stream (host walk by default; on the device with
+ * LPK_GEN_DEVICE_CLOCK; deterministic on the device when the clock has no
+ * random part), the band-overlap gate, the fan-out kernel, AWGN and the rx
+ * chain, handing each chunk to `sink`. `flags` is an OR of the values above. */
 lpk_status lpk_generate_band(lpk_scene *s, int32_t r_idx, int32_t b_idx, uint64_t seed_base,
-                             int32_t work_idx, int64_t chunk_samples, int32_t noise,
+                             int32_t work_idx, int64_t chunk_samples, int32_t flags,
                              lpk_sink_fn sink, void *user, lpk_band_result *result);
 
 /* Stream one band to <dir>/<name>.iq.c64 (raw little-endian complex64,
  * StreamingC64Writer, src/output/mod.rs:100-147). The JSON sidecar is
  * written by the caller, which holds the descriptor. */
 lpk_status lpk_generate_band_to_file(lpk_scene *s, int32_t r_idx, int32_t b_idx, uint64_t seed_base,
-                                     int32_t work_idx, int64_t chunk_samples, int32_t noise,
+                                     int32_t work_idx, int64_t chunk_samples, int32_t flags,
                                      const char *path, lpk_band_result *result);
 
 /* Host clock stream (ClockStream, src/clock/mod.rs:229-347) exposed for

@@ -81,8 +81,13 @@ lpk_status build_dev_band(lpk_ctx *ctx, const lpk_band_desc *d, int64_t i0, int6
     if (n < 0 || i0 < 0) return fail(ctx, LPK_EINVAL, "chunk start and length must be non-negative");
     if (d->rx_kind != LPK_RX_STATIONARY && d->rx_kind != LPK_RX_PER_SAMPLE)
         return fail(ctx, LPK_EINVAL, "unknown rx_kind");
-    if (d->clock_mode != LPK_CLOCK_HOST && d->clock_mode != LPK_CLOCK_DETERMINISTIC)
-        return fail(ctx, LPK_EINVAL, "clock_mode not supported by this entry point");
+    if (d->clock_mode != LPK_CLOCK_HOST && d->clock_mode != LPK_CLOCK_DETERMINISTIC &&
+        d->clock_mode != LPK_CLOCK_DEVICE_WALK)
+        return fail(ctx, LPK_EINVAL, "unknown clock_mode");
+    if (d->clock_mode == LPK_CLOCK_DEVICE_WALK &&
+        (!(d->clock_master_rate_hz > 0.0) || !finite(d->clock_master_rate_hz) || !(d->clock_allan_1s >= 0.0) ||
+         !finite(d->clock_allan_1s)))
+        return fail(ctx, LPK_EINVAL, "device clock walk needs a positive master rate and allan >= 0");
     if (d->n_post < 0 || d->n_post > 3) return fail(ctx, LPK_EINVAL, "n_post must be 0..3");
     b.epoch = d->epoch_unix;
     b.fs = d->fs_hz;
@@ -129,6 +134,95 @@ lpk_status build_dev_band(lpk_ctx *ctx, const lpk_band_desc *d, int64_t i0, int6
     return LPK_OK;
 }
 
+// Master-grid indices [kA, kA + span) the chunk's Δt interpolation reads
+// (one index of margin on each side of what ClockStream::delta_t_at uses).
+int64_t walk_span(const lpk_band_desc *d, int64_t i0, int64_t n, int64_t *kA_out) {
+    const double fs = d->fs_hz, fm = d->clock_master_rate_hz;
+    double x0 = ((double)i0 / fs) * fm;
+    double x1 = ((double)(i0 + (n > 0 ? n - 1 : 0)) / fs) * fm;
+    int64_t kA = x0 <= 0.0 ? 0 : (int64_t)std::floor(x0);
+    int64_t kB = (x1 <= 0.0 ? 0 : (int64_t)std::floor(x1)) + 2;
+    kA = kA > 0 ? kA - 1 : 0;
+    *kA_out = kA;
+    return kB - kA + 1;
+}
+
+lpk_status prepare_walk(lpk_ctx *c, const lpk_band_desc *d, int64_t i0, int64_t n, DevBand &b, double *d_eps,
+                        int64_t eps_cap) {
+    int64_t kA;
+    int64_t span = walk_span(d, i0, n, &kA);
+    if (span > eps_cap) return fail(c, LPK_EINVAL, "walk span exceeds its scratch region");
+    const int64_t kB = kA + span - 1;
+    const double sigma = d->clock_allan_1s / std::sqrt(d->clock_master_rate_hz);  // clock/mod.rs:275
+    WalkState *w = nullptr;
+    for (auto &s : c->walks)
+        if (s.seed == d->clock_seed && s.fm == d->clock_master_rate_hz && s.sigma == sigma) w = &s;
+    if (!w) {
+        c->walks.push_back(WalkState{});
+        w = &c->walks.back();
+        w->seed = d->clock_seed;
+        w->fm = d->clock_master_rate_hz;
+        w->sigma = sigma;
+    }
+    const int64_t need = kB / kWalkBlock;  // carry(need) must be known
+    if (need + 1 > w->cap) {
+        int64_t cap = w->cap ? w->cap : 1024;
+        while (cap < need + 1) cap *= 2;
+        double *tot = nullptr, *car = nullptr;
+        cudaError_t e = cudaMalloc(&tot, sizeof(double) * (size_t)cap);
+        if (e == cudaSuccess) e = cudaMalloc(&car, sizeof(double) * (size_t)(cap + 1));
+        if (e != cudaSuccess) {
+            if (tot) cudaFree(tot);
+            return fail(c, LPK_ENOMEM, "clock walk carry allocation failed");
+        }
+        if (w->nb_done > 0) {
+            cudaMemcpyAsync(tot, w->d_tot, sizeof(double) * (size_t)w->nb_done, cudaMemcpyDeviceToDevice, c->stream);
+            cudaMemcpyAsync(car, w->d_carry, sizeof(double) * (size_t)(w->nb_done + 1), cudaMemcpyDeviceToDevice,
+                            c->stream);
+        }
+        cudaStreamSynchronize(c->stream);
+        if (w->d_tot) cudaFree(w->d_tot);
+        if (w->d_carry) cudaFree(w->d_carry);
+        w->d_tot = tot;
+        w->d_carry = car;
+        w->cap = cap;
+    }
+    cudaError_t e = cudaSuccess;
+    if (need > w->nb_done || (need == 0 && w->nb_done == 0)) {
+        if (w->nb_done == 0) e = cudaMemsetAsync(w->d_carry, 0, sizeof(double), c->stream);
+        if (e == cudaSuccess && need > w->nb_done) {
+            e = launch_walk_totals(w->seed, w->sigma, w->nb_done, need, w->d_tot, w->d_carry, c->stream);
+            c->launches += 2;
+        }
+        if (e != cudaSuccess) return cuda_fail(c, e, "clock walk totals");
+        if (need > w->nb_done) w->nb_done = need;
+    }
+    e = launch_walk_materialize(w->seed, w->sigma, w->d_carry, kA, kB, d_eps, c->stream);
+    c->launches += 1;
+    if (e != cudaSuccess) return cuda_fail(c, e, "clock walk materialisation");
+    b.eps = d_eps;
+    b.eps_k0 = kA;
+    b.fm = d->clock_master_rate_hz;
+    return LPK_OK;
+}
+
+void prof_begin(lpk_ctx *c) {
+    if (!c->profiling) return;
+    if (c->prof_used == c->prof_events.size()) {
+        cudaEvent_t a, b;
+        if (cudaEventCreate(&a) != cudaSuccess) return;
+        if (cudaEventCreate(&b) != cudaSuccess) { cudaEventDestroy(a); return; }
+        c->prof_events.push_back({a, b});
+    }
+    cudaEventRecord(c->prof_events[c->prof_used].first, c->stream);
+}
+
+void prof_end(lpk_ctx *c) {
+    if (!c->profiling || c->prof_used >= c->prof_events.size()) return;
+    cudaEventRecord(c->prof_events[c->prof_used].second, c->stream);
+    ++c->prof_used;
+}
+
 lpk_status check_active(lpk_ctx *ctx, const int32_t *active, int32_t n_active) {
     if (n_active < 0 || n_active > 256) return fail(ctx, LPK_EINVAL, "n_active must be 0..256");
     if (n_active > 0 && !active) return fail(ctx, LPK_EINVAL, "active_tx is NULL");
@@ -154,6 +248,64 @@ const char *lpk_global_last_error(void) {
 }
 
 const char *lpk_last_error(const lpk_ctx *ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+void *lpk_ctx_stream(lpk_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+lpk_status lpk_profile_enable(lpk_ctx *c, int32_t on) {
+    if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
+    c->profiling = on != 0;
+    return LPK_OK;
+}
+
+lpk_status lpk_profile_reset(lpk_ctx *c) {
+    if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
+    cudaStreamSynchronize(c->stream);
+    c->prof_used = 0;
+    c->launches = 0;
+    return LPK_OK;
+}
+
+lpk_status lpk_profile_read(lpk_ctx *c, double *ms, int64_t *fan, int64_t *all) {
+    if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "profile synchronize");
+    double total = 0.0;
+    for (size_t i = 0; i < c->prof_used; ++i) {
+        float t = 0.0f;
+        e = cudaEventElapsedTime(&t, c->prof_events[i].first, c->prof_events[i].second);
+        if (e != cudaSuccess) return cuda_fail(c, e, "profile event");
+        total += t;
+    }
+    if (ms) *ms = total;
+    if (fan) *fan = (int64_t)c->prof_used;
+    if (all) *all = c->launches;
+    return LPK_OK;
+}
+
+lpk_status lpk_probe_fp64_peak(lpk_ctx *c, double *tflops) {
+    if (!c || !tflops) return fail(c, LPK_EINVAL, "NULL argument");
+    cudaSetDevice(c->device);
+    cudaDeviceProp prop;
+    cudaError_t e = cudaGetDeviceProperties(&prop, c->device);
+    if (e != cudaSuccess) return cuda_fail(c, e, "device properties");
+    const int blocks = prop.multiProcessorCount * 8, iters = 1 << 14;
+    lpk_status st = ensure_scratch(c, sizeof(double) * 256 * (size_t)blocks);
+    if (st) return st;
+    double best = 0.0;
+    for (int rep = 0; rep < 4; ++rep) {
+        e = cudaEventRecord(c->ev_start, c->stream);
+        if (e == cudaSuccess) e = launch_fp64_probe((double *)c->d_scratch, blocks, iters, c->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev_stop, c->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(c->ev_stop);
+        float t = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t, c->ev_start, c->ev_stop);
+        if (e != cudaSuccess) return cuda_fail(c, e, "fp64 probe");
+        double flops = 2.0 * 8.0 * (double)iters * 256.0 * (double)blocks;
+        if (rep > 0 && t > 0.0f) best = std::fmax(best, flops / (t * 1e-3) / 1e12);
+    }
+    *tflops = best;
+    return LPK_OK;
+}
 
 lpk_status lpk_ctx_create(lpk_ctx **out, int32_t device) {
     if (!out) return fail(nullptr, LPK_EINVAL, "out is NULL");
@@ -192,6 +344,14 @@ void lpk_ctx_destroy(lpk_ctx *c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     free_scene(c);
+    for (auto &w : c->walks) {
+        if (w.d_tot) cudaFree(w.d_tot);
+        if (w.d_carry) cudaFree(w.d_carry);
+    }
+    for (auto &p : c->prof_events) {
+        cudaEventDestroy(p.first);
+        cudaEventDestroy(p.second);
+    }
     if (c->d_scratch) cudaFree(c->d_scratch);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
     if (c->ev_start) cudaEventDestroy(c->ev_start);
@@ -346,18 +506,28 @@ lpk_status lpk_band_chunk_device(lpk_ctx *c, const lpk_band_desc *band, const in
     b.delta = d_delta;
     b.rxpos = d_rxpos;
     cudaSetDevice(c->device);
-    // active list and unoccluded words live in the small head of the scratch
-    size_t head = align256(sizeof(int32_t) * 256) + align256(sizeof(uint32_t) * 256);
-    if ((st = ensure_scratch(c, head))) return st;
+    // active list, unoccluded words and the clock walk live in the scratch
+    size_t off_uw = align256(sizeof(int32_t) * 256);
+    size_t off_eps = off_uw + align256(sizeof(uint32_t) * 256);
+    int64_t kA = 0, span = b.clock_mode == LPK_CLOCK_DEVICE_WALK ? walk_span(band, i0, n, &kA) : 0;
+    if ((st = ensure_scratch(c, off_eps + align256(sizeof(double) * (size_t)span)))) return st;
     int32_t *d_active = (int32_t *)c->d_scratch;
-    uint32_t *d_uw = (uint32_t *)((char *)c->d_scratch + align256(sizeof(int32_t) * 256));
+    uint32_t *d_uw = (uint32_t *)((char *)c->d_scratch + off_uw);
     cudaError_t e = cudaMemcpyAsync(d_active, active, sizeof(int32_t) * (size_t)n_active, cudaMemcpyHostToDevice,
                                     c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_uw, 0, sizeof(uint32_t) * 256, c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "chunk setup");
+    if (span && (st = prepare_walk(c, band, i0, n, b, (double *)((char *)c->d_scratch + off_eps), span))) return st;
+    prof_begin(c);
     e = launch_band_reference(b, c->d_tx, d_active, n_active, (float2 *)d_out, d_uw, c->stream);
+    prof_end(c);
+    c->launches += n > 0;
     if (e != cudaSuccess) return cuda_fail(c, e, "fan-out kernel launch");
-    (void)d_unocc;
+    if (d_unocc && n_active > 0) {
+        c->launches += 1;
+        e = launch_or_flags(d_uw, d_unocc, n_active, b.has_antenna ? 0 : (n > 0 ? 1 : 2), c->stream);
+        if (e != cudaSuccess) return cuda_fail(c, e, "occlusion flags");
+    }
     return LPK_OK;
 }
 
@@ -387,7 +557,9 @@ lpk_status lpk_band_chunk(lpk_ctx *c, const lpk_band_desc *band, const int32_t *
     size_t off_rx = off_delta + align256(sizeof(double) * n_delta);
     size_t n_rx = b.rx_kind == LPK_RX_PER_SAMPLE ? 3 * (size_t)n : 0;
     size_t off_out = off_rx + align256(sizeof(double) * n_rx);
-    size_t total = off_out + align256(sizeof(float2) * (size_t)n);
+    size_t off_eps = off_out + align256(sizeof(float2) * (size_t)n);
+    int64_t kA = 0, span = b.clock_mode == LPK_CLOCK_DEVICE_WALK ? walk_span(band, i0, n, &kA) : 0;
+    size_t total = off_eps + align256(sizeof(double) * (size_t)span);
     if ((st = ensure_scratch(c, total))) return st;
     char *base = (char *)c->d_scratch;
     int32_t *d_active = (int32_t *)(base + off_active);
@@ -405,7 +577,11 @@ lpk_status lpk_band_chunk(lpk_ctx *c, const lpk_band_desc *band, const int32_t *
     if (e != cudaSuccess) return cuda_fail(c, e, "chunk upload");
     b.delta = d_delta;
     b.rxpos = d_rx;
+    if (span && (st = prepare_walk(c, band, i0, n, b, (double *)(base + off_eps), span))) return st;
+    prof_begin(c);
     e = launch_band_reference(b, c->d_tx, d_active, n_active, d_out, d_uw, c->stream);
+    prof_end(c);
+    c->launches += n > 0;
     if (e != cudaSuccess) return cuda_fail(c, e, "fan-out kernel launch");
     if (n > 0) e = cudaMemcpyAsync(out, d_out, sizeof(float2) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
     uint32_t uw[256];
@@ -478,6 +654,27 @@ lpk_status lpk_tx_contribution(lpk_ctx *c, const lpk_band_desc *band, int32_t tx
     if (e == cudaSuccess && range_out) e = cudaMemcpyAsync(range_out, d_r, bytes, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "transmitter contribution");
+    return LPK_OK;
+}
+
+lpk_status lpk_clock_device_delta(lpk_ctx *c, const lpk_band_desc *band, int64_t i0, int64_t n, double *out) {
+    if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
+    DevBand b;
+    lpk_status st = build_dev_band(c, band, i0, n, b);
+    if (st) return st;
+    if (b.clock_mode == LPK_CLOCK_HOST) return fail(c, LPK_EINVAL, "host clock mode has no device Δt");
+    if (n == 0) return LPK_OK;
+    if (!out) return fail(c, LPK_EINVAL, "delta_out is NULL");
+    cudaSetDevice(c->device);
+    int64_t kA = 0, span = b.clock_mode == LPK_CLOCK_DEVICE_WALK ? walk_span(band, i0, n, &kA) : 0;
+    size_t off_eps = align256(sizeof(double) * (size_t)n);
+    if ((st = ensure_scratch(c, off_eps + align256(sizeof(double) * (size_t)span)))) return st;
+    double *d_out = (double *)c->d_scratch;
+    if (span && (st = prepare_walk(c, band, i0, n, b, (double *)((char *)c->d_scratch + off_eps), span))) return st;
+    cudaError_t e = launch_band_delta(b, d_out, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "device clock");
     return LPK_OK;
 }
 

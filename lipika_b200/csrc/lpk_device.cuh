@@ -59,6 +59,9 @@ struct DevBand {
     double clock_offset, clock_y0;
     const double *delta;                // n (clock mode HOST)
     const double *rxpos;                // (3, n) (rx PER_SAMPLE)
+    const double *eps;                  // walk ε on master indices [eps_k0, ...) (DEVICE_WALK)
+    int64_t eps_k0;
+    double fm;                          // master (walk) rate
     float noise_std;                    // sqrt(P/2) as f32; 0 = no noise
     int32_t has_noise;
     uint64_t noise_seed;
@@ -279,6 +282,18 @@ __device__ __forceinline__ float2 noise_pair(uint64_t seed, int64_t g) {
     float s, c;
     sincosf(ang, &s, &c);
     return make_float2(__fmul_rn(rr, c), __fmul_rn(rr, s));
+}
+
+// One increment σ·z_k of the receiver clock's white-FM walk at master index
+// k: a counter-based normal (Philox block keyed by the clock seed), so any
+// chunking or GPU regenerates the same walk.
+__device__ __forceinline__ double walk_increment(uint64_t seed, int64_t k, double sigma) {
+    uint4 x = philox4x32_10(make_uint4((uint32_t)(uint64_t)k, (uint32_t)((uint64_t)k >> 32), 0x434C4F4Bu, 0u),
+                            make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+    float u1 = __fmul_rn(__fadd_rn((float)(x.x >> 8), 1.0f), 0x1.0p-24f);
+    float u2 = __fmul_rn((float)(x.y >> 8), 0x1.0p-24f);
+    float z = __fmul_rn(sqrtf(__fmul_rn(-2.0f, logf(u1))), cosf(__fmul_rn(6.28318548f, u2)));
+    return __dmul_rn(sigma, (double)z);
 }
 
 // AWGN then PostOp::apply in chain order (channel/mod.rs:323-334,

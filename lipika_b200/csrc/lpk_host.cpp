@@ -606,15 +606,20 @@ lpk_status lpk_scene_band_desc(const lpk_scene *s, int32_t r, int32_t b, uint64_
 }
 
 lpk_status lpk_generate_band(lpk_scene *s, int32_t r, int32_t b, uint64_t seed_base, int32_t work_idx,
-                             int64_t chunk_samples, int32_t noise, lpk_sink_fn sink, void *user,
+                             int64_t chunk_samples, int32_t flags, lpk_sink_fn sink, void *user,
                              lpk_band_result *res) {
     if (!s || !sink) return host_fail(LPK_EINVAL, "NULL scene or sink");
     if (!s->ctx) return host_fail(LPK_EINVAL, "scene was prepared without a context");
     lpk_band_desc d;
     lpk_status st = lpk_scene_band_desc(s, r, b, seed_base, work_idx, &d);
     if (st) return st;
-    if (noise == LPK_NOISE_OFF) d.noise_power_w = 0.0;
+    if (!(flags & LPK_NOISE_ON)) d.noise_power_w = 0.0;
     const RxHost &rx = s->rx[r];
+    // The device walk covers the white-FM part; flicker and moving receivers
+    // (whose positions need Δt on the host) keep the host stream.
+    if ((flags & LPK_GEN_DEVICE_CLOCK) && d.clock_mode == LPK_CLOCK_HOST && rx.stationary &&
+        !(rx.clock.flicker_floor > 0.0))
+        d.clock_mode = LPK_CLOCK_DEVICE_WALK;
     const int64_t n = lpk_scene_band_samples(s, r, b);
     if (chunk_samples < 1) chunk_samples = 1;
     std::vector<int32_t> active(256);
@@ -685,13 +690,13 @@ int32_t file_sink(void *user, const lpk_cf32 *chunk, int64_t n) {
 }  // namespace
 
 lpk_status lpk_generate_band_to_file(lpk_scene *s, int32_t r, int32_t b, uint64_t seed_base, int32_t work_idx,
-                                     int64_t chunk_samples, int32_t noise, const char *path,
+                                     int64_t chunk_samples, int32_t flags, const char *path,
                                      lpk_band_result *res) {
     if (!path) return host_fail(LPK_EINVAL, "path is NULL");
     FILE *f = fopen(path, "wb");
     if (!f) return host_fail(LPK_EINVAL, std::string("cannot create ") + path + ": " + strerror(errno));
     FileSink fs{f};
-    lpk_status st = lpk_generate_band(s, r, b, seed_base, work_idx, chunk_samples, noise, file_sink, &fs, res);
+    lpk_status st = lpk_generate_band(s, r, b, seed_base, work_idx, chunk_samples, flags, file_sink, &fs, res);
     if (fclose(f) != 0 && !st) st = host_fail(LPK_EINVAL, "closing the IQ file failed");
     return st;
 }

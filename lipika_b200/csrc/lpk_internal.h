@@ -9,8 +9,22 @@
 #include "../../include/lipika_cuda.h"
 #include "lpk_device.cuh"
 
+namespace lpk {
+constexpr int64_t kWalkBlock = 4096;  // master samples per clock-walk scan block
+
+// Cached carries of one receiver clock walk (seed, master rate, step σ).
+struct WalkState {
+    uint64_t seed = 0;
+    double fm = 0.0, sigma = 0.0;
+    int64_t nb_done = 0;   // blocks whose totals and carries are known
+    int64_t cap = 0;
+    double *d_tot = nullptr, *d_carry = nullptr;
+};
+}  // namespace lpk
+
 struct lpk_ctx {
     int device = 0;
+    std::vector<lpk::WalkState> walks;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
     std::string err;
@@ -25,8 +39,11 @@ struct lpk_ctx {
     // pinned host staging
     void *h_pinned = nullptr;
     size_t pinned_bytes = 0;
-    // last kernel time (ms) of the fan-out, for profiling hooks
-    float last_kernel_ms = 0.0f;
+    // measurement hooks
+    bool profiling = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+    size_t prof_used = 0;
+    int64_t launches = 0;
 };
 
 namespace lpk {
@@ -44,6 +61,21 @@ cudaError_t launch_band_reference(const DevBand &b, const DevTx *d_tx, const int
 cudaError_t launch_tx_contribution(const DevBand &b, const DevTx *d_tx, int32_t tx, float2 *d_out,
                                    double *d_phase, double *d_temit, double *d_range, cudaStream_t s);
 cudaError_t launch_rx_chain(const DevBand &b, float2 *d_iq, cudaStream_t s);
+cudaError_t launch_band_delta(const DevBand &b, double *d_out, cudaStream_t s);
+cudaError_t launch_or_flags(const uint32_t *d_uw, uint8_t *d_unocc, int32_t n_active, int mode, cudaStream_t s);
+cudaError_t launch_walk_totals(uint64_t seed, double sigma, int64_t b_from, int64_t b_to, double *d_tot,
+                               double *d_carry, cudaStream_t s);
+cudaError_t launch_walk_materialize(uint64_t seed, double sigma, const double *d_carry, int64_t kA, int64_t kB,
+                                    double *d_eps, cudaStream_t s);
+// Device walk for a band chunk: ensure carries, materialise ε over the
+// chunk's master range into `eps_region` of the scratch (lpk_abi.cu).
+lpk_status prepare_walk(lpk_ctx *ctx, const lpk_band_desc *d, int64_t i0, int64_t n, DevBand &b, double *d_eps,
+                        int64_t eps_cap);
+int64_t walk_span(const lpk_band_desc *d, int64_t i0, int64_t n, int64_t *kA);
+// Record a profiling event pair around a fan-out launch (no-op when off).
+void prof_begin(lpk_ctx *ctx);
+void prof_end(lpk_ctx *ctx);
+cudaError_t launch_fp64_probe(double *d_out, int blocks, int iters, cudaStream_t s);
 cudaError_t launch_solve(const DevTx *d_tx, int32_t tx, const double *d_obs, const double *d_t, int64_t n,
                          double epoch, int32_t iterations, double inv_c, double *d_temit, double *d_range,
                          cudaStream_t s);

@@ -17,6 +17,16 @@ constexpr int kBlock = 256;
 __device__ __forceinline__ double band_delta(const DevBand &b, int64_t j, double t_local) {
     if (b.clock_mode == LPK_CLOCK_DETERMINISTIC)  // (ε=0 + flicker=0) + c + m·t, clock/mod.rs:311-345
         return __dadd_rn(0.0, __dadd_rn(b.clock_offset, __dmul_rn(b.clock_y0, t_local)));
+    if (b.clock_mode == LPK_CLOCK_DEVICE_WALK) {  // ClockStream::delta_t_at, clock/mod.rs:329-346
+        double x = __dmul_rn(t_local, b.fm);      // elapsed = t - 0.0
+        if (x <= 0.0)
+            return __dadd_rn(__dadd_rn(b.eps[0 - b.eps_k0], 0.0), __dadd_rn(b.clock_offset, __dmul_rn(b.clock_y0, 0.0)));
+        int64_t k0 = floor_to_i64(x);
+        double frac = __dsub_rn(x, (double)k0);
+        double lo = b.eps[k0 - b.eps_k0], hi = b.eps[k0 + 1 - b.eps_k0];
+        double eps = __dadd_rn(__dmul_rn(lo, __dsub_rn(1.0, frac)), __dmul_rn(hi, frac));
+        return __dadd_rn(__dadd_rn(eps, 0.0), __dadd_rn(b.clock_offset, __dmul_rn(b.clock_y0, t_local)));
+    }
     return b.delta[j];
 }
 
@@ -147,9 +157,131 @@ k_rx_chain(const DevBand b, float2 *__restrict__ iq) {
     iq[j] = band_epilogue(b, v.x, v.y, b.i0 + j);
 }
 
+// ---------------------------------------------------------------- clock walk
+// The walk ε(k) = Σ_{j<=k} σ z_j is defined through fixed scan blocks of
+// kWalkBlock master samples: ε(k) = carry(b) + P_b(k), with P_b the in-block
+// inclusive prefix computed by one fixed parallel order and carry(b) the
+// sequential sum of the totals of blocks 0..b-1. Nothing depends on how the
+// band is chunked, so every chunking reproduces the same ε.
+constexpr int kWalkThreads = 256;
+constexpr int kWalkPer = kWalkBlock / kWalkThreads;  // 16
+
+__global__ void __launch_bounds__(kWalkThreads)
+k_walk_block(uint64_t seed, double sigma, int64_t b0, double *__restrict__ totals,
+             const double *__restrict__ carry, double *__restrict__ eps, int64_t kA, int64_t kB) {
+    __shared__ double warp_tot[kWalkThreads / 32];
+    const int64_t b = b0 + blockIdx.x;
+    const int64_t base = b * kWalkBlock + (int64_t)threadIdx.x * kWalkPer;
+    double v[kWalkPer];
+    double run = 0.0;
+#pragma unroll
+    for (int i = 0; i < kWalkPer; ++i) {
+        run = __dadd_rn(run, walk_increment(seed, base + i, sigma));
+        v[i] = run;
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double incl = run;  // warp inclusive scan of per-thread totals
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        double o = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl = __dadd_rn(o, incl);
+    }
+    if (lane == 31) warp_tot[wid] = incl;
+    __syncthreads();
+    double wpre = 0.0;
+    for (int w = 0; w < wid; ++w) wpre = __dadd_rn(wpre, warp_tot[w]);
+    const double offset = __dadd_rn(wpre, __dsub_rn(incl, run));  // exclusive prefix of this thread
+    if (totals) {
+        if (threadIdx.x == kWalkThreads - 1) totals[b] = __dadd_rn(offset, v[kWalkPer - 1]);
+        return;
+    }
+    const double c = carry[b];
+#pragma unroll
+    for (int i = 0; i < kWalkPer; ++i) {
+        int64_t k = base + i;
+        if (k >= kA && k <= kB) eps[k - kA] = __dadd_rn(c, __dadd_rn(offset, v[i]));
+    }
+}
+
+// carry(b + 1) = carry(b) + total(b), sequentially, for the new blocks.
+__global__ void k_walk_carry(const double *__restrict__ totals, double *__restrict__ carry, int64_t b_from,
+                             int64_t b_to) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (b_from == 0) carry[0] = 0.0;
+    double c = carry[b_from];
+    for (int64_t b = b_from; b < b_to; ++b) {
+        c = __dadd_rn(c, totals[b]);
+        carry[b + 1] = c;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_band_delta(const DevBand b, double *__restrict__ out) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= b.n) return;
+    out[j] = band_delta(b, j, __ddiv_rn((double)(b.i0 + j), b.fs));
+}
+
+// unoccluded[k] |= flag: from the kernel's per-transmitter words (mode 0),
+// or "at least one sample" without an antenna (mode 1), or nothing (mode 2).
+__global__ void k_or_flags(const uint32_t *__restrict__ uw, uint8_t *__restrict__ unocc, int32_t n_active,
+                           int mode) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n_active) return;
+    uint8_t f = mode == 0 ? (uint8_t)(uw[k] != 0) : (uint8_t)(mode == 1);
+    unocc[k] |= f;
+}
+
 inline unsigned grid_for(int64_t n) { return (unsigned)((n + kBlock - 1) / kBlock); }
 
 }  // namespace
+
+namespace {
+// Eight independent DFMA chains per thread, all in registers: issue-bound on
+// the FP64 pipe. The result is stored so nothing is optimised away.
+__global__ void __launch_bounds__(256) k_fp64_probe(double *out, int iters) {
+    double a = 1.0 + threadIdx.x * 1e-9, b = 0.999999, c = 1e-7;
+    double x0 = a, x1 = a + 1, x2 = a + 2, x3 = a + 3, x4 = a + 4, x5 = a + 5, x6 = a + 6, x7 = a + 7;
+    for (int i = 0; i < iters; ++i) {
+        x0 = fma(x0, b, c); x1 = fma(x1, b, c); x2 = fma(x2, b, c); x3 = fma(x3, b, c);
+        x4 = fma(x4, b, c); x5 = fma(x5, b, c); x6 = fma(x6, b, c); x7 = fma(x7, b, c);
+    }
+    out[blockIdx.x * blockDim.x + threadIdx.x] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+}
+}  // namespace
+
+cudaError_t launch_fp64_probe(double *d_out, int blocks, int iters, cudaStream_t s) {
+    k_fp64_probe<<<blocks, 256, 0, s>>>(d_out, iters);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_band_delta(const DevBand &b, double *d_out, cudaStream_t s) {
+    if (b.n <= 0) return cudaSuccess;
+    k_band_delta<<<grid_for(b.n), kBlock, 0, s>>>(b, d_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_or_flags(const uint32_t *d_uw, uint8_t *d_unocc, int32_t n_active, int mode, cudaStream_t s) {
+    k_or_flags<<<1, 256, 0, s>>>(d_uw, d_unocc, n_active, mode);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_walk_totals(uint64_t seed, double sigma, int64_t b_from, int64_t b_to, double *d_tot,
+                               double *d_carry, cudaStream_t s) {
+    if (b_to <= b_from) return cudaSuccess;
+    k_walk_block<<<(unsigned)(b_to - b_from), kWalkThreads, 0, s>>>(seed, sigma, b_from, d_tot, nullptr, nullptr, 0, -1);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_walk_carry<<<1, 32, 0, s>>>(d_tot, d_carry, b_from, b_to);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_walk_materialize(uint64_t seed, double sigma, const double *d_carry, int64_t kA, int64_t kB,
+                                    double *d_eps, cudaStream_t s) {
+    if (kB < kA) return cudaSuccess;
+    int64_t b0 = kA / kWalkBlock, b1 = kB / kWalkBlock;
+    k_walk_block<<<(unsigned)(b1 - b0 + 1), kWalkThreads, 0, s>>>(seed, sigma, b0, nullptr, d_carry, d_eps, kA, kB);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_band_reference(const DevBand &b, const DevTx *d_tx, const int32_t *d_active,
                                   int32_t n_active, float2 *d_out, uint32_t *d_unocc, cudaStream_t s) {

@@ -28,7 +28,7 @@ LPK_CLOCK_HOST, LPK_CLOCK_DETERMINISTIC, LPK_CLOCK_DEVICE_WALK = 0, 1, 2
 LPK_RX_STATIONARY, LPK_RX_PER_SAMPLE = 0, 1
 LPK_POST_GAIN, LPK_POST_NONLINEARITY, LPK_POST_ADC = 0, 1, 2
 LPK_SOLVER_REFERENCE, LPK_SOLVER_SPLIT = 0, 1
-LPK_NOISE_OFF, LPK_NOISE_ON = 0, 1
+LPK_NOISE_OFF, LPK_NOISE_ON, LPK_GEN_DEVICE_CLOCK = 0, 1, 2
 
 
 class LpkError(RuntimeError):
@@ -103,6 +103,11 @@ SIGNATURES = {
     "lpk_last_error": (C.c_char_p, [_VP]),
     "lpk_global_last_error": (C.c_char_p, []),
     "lpk_version": (C.c_char_p, []),
+    "lpk_ctx_stream": (_VP, [_VP]),
+    "lpk_profile_enable": (C.c_int32, [_VP, C.c_int32]),
+    "lpk_profile_reset": (C.c_int32, [_VP]),
+    "lpk_profile_read": (C.c_int32, [_VP, _D, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "lpk_probe_fp64_peak": (C.c_int32, [_VP, _D]),
     "lpk_scene_upload": (C.c_int32, [_VP, C.POINTER(TxDesc), C.c_int32]),
     "lpk_band_chunk": (C.c_int32, [_VP, C.POINTER(BandDesc), _I32, C.c_int32, C.c_int64, C.c_int64, _D, _D, _CF, _U8]),
     "lpk_band_chunk_device": (C.c_int32, [_VP, C.POINTER(BandDesc), _I32, C.c_int32, C.c_int64, C.c_int64,
@@ -111,6 +116,7 @@ SIGNATURES = {
     "lpk_solve_emission_times": (C.c_int32, [_VP, C.c_int32, _D, _D, C.c_int64, C.c_double, C.c_int32, _D, _D]),
     "lpk_tx_contribution": (C.c_int32, [_VP, C.POINTER(BandDesc), C.c_int32, C.c_int64, C.c_int64, _D, _D, _CF,
                                         _D, _D, _D]),
+    "lpk_clock_device_delta": (C.c_int32, [_VP, C.POINTER(BandDesc), C.c_int64, C.c_int64, _D]),
     "lpk_rx_chain_apply": (C.c_int32, [_VP, C.POINTER(BandDesc), _CF, C.c_int64]),
     "lpk_scene_prepare": (C.c_int32, [_VP, C.POINTER(A.SceneCfg), C.POINTER(_VP)]),
     "lpk_scene_free": (None, [_VP]),

@@ -142,8 +142,12 @@ class Prepared:
         return d
 
     def generate_band(self, r: int, b: int, seed: int, work_idx: int, chunk_samples: int,
-                      sink: Callable[[np.ndarray], bool], noise: bool = True) -> N.BandResult:
-        """generate_band (src/pipeline.rs:836-1019); `sink(chunk)` returns True to stop."""
+                      sink: Callable[[np.ndarray], bool], noise: bool = True,
+                      device_clock: bool = False) -> N.BandResult:
+        """generate_band (src/pipeline.rs:836-1019); `sink(chunk)` returns True to stop.
+
+        device_clock=True draws the receiver's white-FM walk on the GPU
+        (counter-based, moment-matched) instead of the host stream."""
         err: list = []
 
         def _sink(_user, ptr, n):
@@ -156,8 +160,9 @@ class Prepared:
 
         cb = N.SINK_FN(_sink)
         res = N.BandResult()
+        flags = (N.LPK_NOISE_ON if noise else N.LPK_NOISE_OFF) | (N.LPK_GEN_DEVICE_CLOCK if device_clock else 0)
         code = N.lib().lpk_generate_band(self.h, r, b, seed & 0xFFFFFFFFFFFFFFFF, work_idx, max(1, chunk_samples),
-                                         N.LPK_NOISE_ON if noise else N.LPK_NOISE_OFF, cb, None, C.byref(res))
+                                         flags, cb, None, C.byref(res))
         if err:
             raise err[0]
         N.check(code, self.ctx.h)
