@@ -185,6 +185,22 @@ lpk_status lpk_band_chunk_device(lpk_ctx *ctx, const lpk_band_desc *band, const 
                                  const double *d_rx_pos3n, lpk_cf32 *d_out, uint8_t *d_unoccluded);
 lpk_status lpk_sync(lpk_ctx *ctx);
 
+/* lpk_band_chunk_device for callers that cannot allocate device memory when
+ * they render (a real-time thread that must not stall on the CUDA allocator,
+ * a host that reserved the device for its own pool). No counterpart in the
+ * reference. It calls no cudaMalloc/cudaFree: its working memory is one
+ * file-scope static device array of 10 MiB that every GPU loading this
+ * library holds until exit. Limits: at most 256 active transmitters; with
+ * LPK_CLOCK_DEVICE_WALK a chunk may span at most 2^20 master-clock samples
+ * and lie within the first 2^29 (larger requests return LPK_EINVAL). The
+ * first call on a device looks up the array's address (cudaGetSymbolAddress)
+ * — make that first call before any stream capture. All calls share the
+ * array: calls that overlap on the GPU race; each call re-clears what it
+ * needs zeroed. Outputs equal lpk_band_chunk_device's. */
+lpk_status lpk_band_chunk_device_static(lpk_ctx *ctx, const lpk_band_desc *band, const int32_t *active_tx,
+                                        int32_t n_active, int64_t i0, int64_t n, const double *d_delta_t,
+                                        const double *d_rx_pos3n, lpk_cf32 *d_out, uint8_t *d_unoccluded);
+
 /* Per-transmitter emission solve (channel/mod.rs:106-121,
  * solve_emission_times): `iterations` fixed-point steps from t - 70 ms.
  * All arrays host memory, obs3n is (3, n) axis-major. */

@@ -113,6 +113,8 @@ SIGNATURES = {
     "lpk_band_chunk_device": (C.c_int32, [_VP, C.POINTER(BandDesc), _I32, C.c_int32, C.c_int64, C.c_int64,
                                           _VP, _VP, _VP, _VP]),
     "lpk_sync": (C.c_int32, [_VP]),
+    "lpk_band_chunk_device_static": (C.c_int32, [_VP, C.POINTER(BandDesc), _I32, C.c_int32, C.c_int64, C.c_int64,
+                                                 _VP, _VP, _VP, _VP]),
     "lpk_solve_emission_times": (C.c_int32, [_VP, C.c_int32, _D, _D, C.c_int64, C.c_double, C.c_int32, _D, _D]),
     "lpk_tx_contribution": (C.c_int32, [_VP, C.POINTER(BandDesc), C.c_int32, C.c_int64, C.c_int64, _D, _D, _CF,
                                         _D, _D, _D]),
