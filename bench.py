@@ -57,6 +57,9 @@ def _args():
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU time of the baseline sample")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--solver", default="split", choices=["split", "reference"],
+                   help="fan-out path timed for `value` (the plain FP64 kernel is timed beside split)")
+    p.add_argument("--plain-steps", type=int, default=5, help="steps of the plain FP64 kernel (0: skip)")
     return p.parse_args()
 
 
@@ -137,10 +140,10 @@ def _dist():
     return ws, rank, local
 
 
-def _traffic_from_profile(launch_band_samples: float):
-    """DRAM bytes per launch from the committed ncu summary (scaled by band
-    samples per launch), or None."""
-    path = os.path.join(ROOT, "profiles", "fanout_traffic.json")
+def _traffic_from_profile(launch_band_samples: float, solver: str):
+    """DRAM bytes per launch from the committed ncu summary of this solver's
+    fan-out (scaled by band samples per launch), or None."""
+    path = os.path.join(ROOT, "profiles", f"fanout_traffic_{solver}.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:
@@ -237,6 +240,7 @@ def run_ours(a):
         d = prep.band_desc(r, b, seed, w)
         if d.clock_mode == N.LPK_CLOCK_HOST:
             d.clock_mode = N.LPK_CLOCK_DEVICE_WALK
+        d.solver = N.LPK_SOLVER_SPLIT if a.solver == "split" else N.LPK_SOLVER_REFERENCE
         act = prep.active(r, b)
         out = torch.empty(2 * n, dtype=torch.float32, device=f"cuda:{local}")
         bands.append((d, (C.c_int32 * max(len(act), 1))(*act), len(act), n, out))
@@ -284,6 +288,30 @@ def run_ours(a):
         ms = float(t.item())
     value = total_txrx * a.steps * ws / (ms * 1e-3)
 
+    # the plain all-FP64 kernel on the same scene (the metric's comparison)
+    plain = None
+    if a.solver == "split" and a.plain_steps > 0:
+        for d, *_ in bands:
+            d.solver = N.LPK_SOLVER_REFERENCE
+        step()
+        barrier()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for _ in range(a.plain_steps):
+            step()
+        p1.record(stream)
+        p1.synchronize()
+        pms = p0.elapsed_time(p1)
+        if dist is not None:
+            t = torch.tensor([pms], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            pms = float(t.item())
+        for d, *_ in bands:
+            d.solver = N.LPK_SOLVER_SPLIT
+        plain = {"value": total_txrx * a.plain_steps * ws / (pms * 1e-3), "unit": UNIT,
+                 "ms_per_step": pms / a.plain_steps, "steps": a.plain_steps,
+                 "kernel": "k_band_reference (reference semantics, all FP64)"}
+
     # roofline of the dominant kernel (the fan-out), from its own events
     avg_launch_ms = fan_ms.value / max(fan_n.value, 1)
     txrx_per_launch = total_txrx * a.steps / max(fan_n.value, 1)
@@ -297,7 +325,7 @@ def run_ours(a):
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     hbm_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
-    traffic = _traffic_from_profile(band_per_launch)
+    traffic = _traffic_from_profile(band_per_launch, a.solver)
     achieved_gbs = BYTES_PER_BAND_SAMPLE * band_per_launch / (avg_launch_ms * 1e-3) / 1e9
 
     # e2e through the host-level C ABI, host buffers
@@ -325,7 +353,9 @@ def run_ours(a):
                 pos[0] = 0
                 res = N.BandResult()
                 N.check(L.lpk_generate_band(p2.h, r, b, seed, w, P.DEFAULT_CHUNK_SAMPLES,
-                                            N.LPK_NOISE_ON | N.LPK_GEN_DEVICE_CLOCK, cb, None, C.byref(res)),
+                                            N.LPK_NOISE_ON | N.LPK_GEN_DEVICE_CLOCK
+                                            | (N.LPK_GEN_SPLIT if a.solver == "split" else 0),
+                                            cb, None, C.byref(res)),
                         ctx.h)
             p2.close()
 
@@ -363,13 +393,17 @@ def run_ours(a):
         "dtype": "f64", "data": "synthetic (seeded scene, no dataset)",
         "config": {"workload": WORKLOAD, "duration_s": a.duration, "tx_rx_samples_per_step_per_gpu": total_txrx,
                    "band_samples_per_step_per_gpu": total_band, "chunk_samples": a.chunk,
-                   "solver": "reference semantics: 2 fixed-point iterations from t-70 ms, all FP64",
+                   "solver": ("split precision: FP64 anchors per 1024-sample tile (reference 2-iteration solve), "
+                              "quadratic delay per sample, FP64 phase reduction, FP32 sin/cos and MAC; "
+                              "indices bit-exact via guard-band fallback") if a.solver == "split" else
+                             "reference semantics: 2 fixed-point iterations from t-70 ms, all FP64",
                    "clock": "white-FM walk generated on the device", "noise": "AWGN on",
                    "parallelism": f"{ws} GPU(s), one scene replica per GPU",
                    "l2": "output (1.97 GB/step) is larger than L2; scene tables (~3 MB) are L2-resident by design"},
         "roofline": {"bound": "fp64", "achieved": achieved_tf, "peak": peak_fp64.value, "unit": "TFLOP/s",
                      "frac": achieved_tf / peak_fp64.value if peak_fp64.value else None,
-                     "traffic": traffic, "kernel": "k_band_reference",
+                     "traffic": traffic,
+                     "kernel": "k_split_anchor + k_band_split" if a.solver == "split" else "k_band_reference",
                      "basis": f"{FLOP_PER_SAMPLE} FP64-equivalent flop per tx·rx sample x {txrx_per_launch:.4g} "
                               f"tx·rx samples per launch / {avg_launch_ms:.3f} ms average launch (CUDA events "
                               "on the launching stream); peak = FP64 DFMA probe measured in this run",
@@ -377,6 +411,8 @@ def run_ours(a):
                              "frac": achieved_gbs / hbm_peak, "peak_source": hbm_src,
                              "algorithmic_bytes_per_launch": BYTES_PER_BAND_SAMPLE * band_per_launch}},
         "e2e": e2e, "gpu_launches": int(all_n.value), "clocks": clk,
+        "plain_fp64": plain,
+        "speedup_vs_plain_fp64": (value / plain["value"]) if plain else None,
     }
     if base is not None:
         line["cpu_baseline"] = base

@@ -268,8 +268,10 @@ typedef struct lpk_band_result {
 enum {
     LPK_NOISE_OFF = 0,          /* no AWGN (deterministic comparisons) */
     LPK_NOISE_ON = 1,           /* AWGN at the band's noise power */
-    LPK_GEN_DEVICE_CLOCK = 2    /* white-FM walk generated on the GPU (counter-based,
+    LPK_GEN_DEVICE_CLOCK = 2,   /* white-FM walk generated on the GPU (counter-based,
                                    moment-matched) instead of the host stream */
+    LPK_GEN_SPLIT = 4           /* split-precision fan-out (LPK_SOLVER_SPLIT) where the
+                                   band allows it (stationary receiver, no antenna) */
 };
 
 /* generate_band (src/pipeline.rs:836-1019) on the GPU: the chunk loop with

@@ -510,7 +510,10 @@ lpk_status lpk_band_chunk_device(lpk_ctx *c, const lpk_band_desc *band, const in
     size_t off_uw = align256(sizeof(int32_t) * 256);
     size_t off_eps = off_uw + align256(sizeof(uint32_t) * 256);
     int64_t kA = 0, span = b.clock_mode == LPK_CLOCK_DEVICE_WALK ? walk_span(band, i0, n, &kA) : 0;
-    if ((st = ensure_scratch(c, off_eps + align256(sizeof(double) * (size_t)span)))) return st;
+    const bool split = use_split(band);
+    size_t off_recs = off_eps + align256(sizeof(double) * (size_t)span);
+    size_t recs = split ? align256(split_recs_bytes(i0, n, n_active)) : 0;
+    if ((st = ensure_scratch(c, off_recs + recs))) return st;
     int32_t *d_active = (int32_t *)c->d_scratch;
     uint32_t *d_uw = (uint32_t *)((char *)c->d_scratch + off_uw);
     cudaError_t e = cudaMemcpyAsync(d_active, active, sizeof(int32_t) * (size_t)n_active, cudaMemcpyHostToDevice,
@@ -519,9 +522,13 @@ lpk_status lpk_band_chunk_device(lpk_ctx *c, const lpk_band_desc *band, const in
     if (e != cudaSuccess) return cuda_fail(c, e, "chunk setup");
     if (span && (st = prepare_walk(c, band, i0, n, b, (double *)((char *)c->d_scratch + off_eps), span))) return st;
     prof_begin(c);
-    e = launch_band_reference(b, c->d_tx, d_active, n_active, (float2 *)d_out, d_uw, c->stream);
+    if (split)
+        e = launch_band_split(b, c->d_tx, d_active, n_active, (char *)c->d_scratch + off_recs, (float2 *)d_out,
+                              nullptr, nullptr, nullptr, c->stream);
+    else
+        e = launch_band_reference(b, c->d_tx, d_active, n_active, (float2 *)d_out, d_uw, c->stream);
     prof_end(c);
-    c->launches += n > 0;
+    c->launches += (n > 0) * (split ? 2 : 1);
     if (e != cudaSuccess) return cuda_fail(c, e, "fan-out kernel launch");
     if (d_unocc && n_active > 0) {
         c->launches += 1;
@@ -559,7 +566,9 @@ lpk_status lpk_band_chunk(lpk_ctx *c, const lpk_band_desc *band, const int32_t *
     size_t off_out = off_rx + align256(sizeof(double) * n_rx);
     size_t off_eps = off_out + align256(sizeof(float2) * (size_t)n);
     int64_t kA = 0, span = b.clock_mode == LPK_CLOCK_DEVICE_WALK ? walk_span(band, i0, n, &kA) : 0;
-    size_t total = off_eps + align256(sizeof(double) * (size_t)span);
+    const bool split = use_split(band);
+    size_t off_recs = off_eps + align256(sizeof(double) * (size_t)span);
+    size_t total = off_recs + (split ? align256(split_recs_bytes(i0, n, n_active)) : 0);
     if ((st = ensure_scratch(c, total))) return st;
     char *base = (char *)c->d_scratch;
     int32_t *d_active = (int32_t *)(base + off_active);
@@ -579,9 +588,13 @@ lpk_status lpk_band_chunk(lpk_ctx *c, const lpk_band_desc *band, const int32_t *
     b.rxpos = d_rx;
     if (span && (st = prepare_walk(c, band, i0, n, b, (double *)(base + off_eps), span))) return st;
     prof_begin(c);
-    e = launch_band_reference(b, c->d_tx, d_active, n_active, d_out, d_uw, c->stream);
+    if (split)
+        e = launch_band_split(b, c->d_tx, d_active, n_active, base + off_recs, d_out, nullptr, nullptr, nullptr,
+                              c->stream);
+    else
+        e = launch_band_reference(b, c->d_tx, d_active, n_active, d_out, d_uw, c->stream);
     prof_end(c);
-    c->launches += n > 0;
+    c->launches += (n > 0) * (split ? 2 : 1);
     if (e != cudaSuccess) return cuda_fail(c, e, "fan-out kernel launch");
     if (n > 0) e = cudaMemcpyAsync(out, d_out, sizeof(float2) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
     uint32_t uw[256];
@@ -633,7 +646,12 @@ lpk_status lpk_tx_contribution(lpk_ctx *c, const lpk_band_desc *band, int32_t tx
     if (!out) return fail(c, LPK_EINVAL, "out is NULL");
     cudaSetDevice(c->device);
     size_t bytes = sizeof(double) * (size_t)n;
-    lpk_status s2 = ensure_scratch(c, 8 * bytes + 4096);
+    const bool split = use_split(band);
+    int64_t kA = 0, span = b.clock_mode == LPK_CLOCK_DEVICE_WALK ? walk_span(band, i0, n, &kA) : 0;
+    size_t off_act = 8 * bytes;
+    size_t off_eps = off_act + 256;
+    size_t off_recs = off_eps + align256(sizeof(double) * (size_t)span);
+    lpk_status s2 = ensure_scratch(c, off_recs + (split ? align256(split_recs_bytes(i0, n, 1)) : 0) + 256);
     if (s2) return s2;
     double *d_delta = (double *)c->d_scratch;
     double *d_rx = d_delta + n;
@@ -641,19 +659,32 @@ lpk_status lpk_tx_contribution(lpk_ctx *c, const lpk_band_desc *band, int32_t tx
     double *d_te = d_phase + n;
     double *d_r = d_te + n;
     float2 *d_out = (float2 *)(d_r + n);
+    char *base = (char *)c->d_scratch;
     cudaError_t e = cudaSuccess;
     if (b.clock_mode == LPK_CLOCK_HOST) e = cudaMemcpyAsync(d_delta, delta_t, bytes, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess && b.rx_kind == LPK_RX_PER_SAMPLE)
         e = cudaMemcpyAsync(d_rx, rx_pos3n, 3 * bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(base + off_act, &tx, sizeof(int32_t), cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "transmitter contribution upload");
     b.delta = d_delta;
     b.rxpos = d_rx;
-    if (e == cudaSuccess) e = launch_tx_contribution(b, c->d_tx, tx, d_out, d_phase, d_te, d_r, c->stream);
+    if (span && (s2 = prepare_walk(c, band, i0, n, b, (double *)(base + off_eps), span))) return s2;
+    if (split) {
+        b.has_noise = 0;  // the contribution alone, as transmitter_contribution_at_receiver returns it
+        b.n_post = 0;
+        e = launch_band_split(b, c->d_tx, (const int32_t *)(base + off_act), 1, base + off_recs, d_out, d_phase, d_te,
+                              d_r, c->stream);
+    } else {
+        e = launch_tx_contribution(b, c->d_tx, tx, d_out, d_phase, d_te, d_r, c->stream);
+    }
     if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, sizeof(float2) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess && phase_out) e = cudaMemcpyAsync(phase_out, d_phase, bytes, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess && t_emit_out) e = cudaMemcpyAsync(t_emit_out, d_te, bytes, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess && range_out) e = cudaMemcpyAsync(range_out, d_r, bytes, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "transmitter contribution");
+    if (split && range_out)  // the split kernel reports delay; range = c · delay
+        for (int64_t i = 0; i < n; ++i) range_out[i] *= kSpeedOfLight;
     return LPK_OK;
 }
 

@@ -614,6 +614,7 @@ lpk_status lpk_generate_band(lpk_scene *s, int32_t r, int32_t b, uint64_t seed_b
     lpk_status st = lpk_scene_band_desc(s, r, b, seed_base, work_idx, &d);
     if (st) return st;
     if (!(flags & LPK_NOISE_ON)) d.noise_power_w = 0.0;
+    if (flags & LPK_GEN_SPLIT) d.solver = LPK_SOLVER_SPLIT;
     const RxHost &rx = s->rx[r];
     // The device walk covers the white-FM part; flicker and moving receivers
     // (whose positions need Δt on the host) keep the host stream.

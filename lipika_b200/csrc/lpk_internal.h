@@ -62,6 +62,17 @@ cudaError_t launch_tx_contribution(const DevBand &b, const DevTx *d_tx, int32_t 
                                    double *d_phase, double *d_temit, double *d_range, cudaStream_t s);
 cudaError_t launch_rx_chain(const DevBand &b, float2 *d_iq, cudaStream_t s);
 cudaError_t launch_band_delta(const DevBand &b, double *d_out, cudaStream_t s);
+// Split-precision fan-out (anchor kernel + per-sample kernel); d_recs holds
+// split_recs_bytes(n, n_active) bytes. The dbg arrays (single transmitter
+// only, may be NULL) receive the reduced phase, emission time and delay.
+size_t split_recs_bytes(int64_t i0, int64_t n, int32_t n_active);
+cudaError_t launch_band_split(const DevBand &b, const DevTx *d_tx, const int32_t *d_active, int32_t n_active,
+                              void *d_recs, float2 *d_out, double *dbg_phase, double *dbg_temit, double *dbg_delay,
+                              cudaStream_t s);
+// True when the band can take the split path (stationary receiver, no antenna).
+inline bool use_split(const lpk_band_desc *d) {
+    return d->solver == LPK_SOLVER_SPLIT && d->rx_kind == LPK_RX_STATIONARY && !d->has_antenna;
+}
 cudaError_t launch_or_flags(const uint32_t *d_uw, uint8_t *d_unocc, int32_t n_active, int mode, cudaStream_t s);
 cudaError_t launch_walk_totals(uint64_t seed, double sigma, int64_t b_from, int64_t b_to, double *d_tot,
                                double *d_carry, cudaStream_t s);

@@ -28,7 +28,7 @@ LPK_CLOCK_HOST, LPK_CLOCK_DETERMINISTIC, LPK_CLOCK_DEVICE_WALK = 0, 1, 2
 LPK_RX_STATIONARY, LPK_RX_PER_SAMPLE = 0, 1
 LPK_POST_GAIN, LPK_POST_NONLINEARITY, LPK_POST_ADC = 0, 1, 2
 LPK_SOLVER_REFERENCE, LPK_SOLVER_SPLIT = 0, 1
-LPK_NOISE_OFF, LPK_NOISE_ON, LPK_GEN_DEVICE_CLOCK = 0, 1, 2
+LPK_NOISE_OFF, LPK_NOISE_ON, LPK_GEN_DEVICE_CLOCK, LPK_GEN_SPLIT = 0, 1, 2, 4
 
 
 class LpkError(RuntimeError):

@@ -143,7 +143,7 @@ class Prepared:
 
     def generate_band(self, r: int, b: int, seed: int, work_idx: int, chunk_samples: int,
                       sink: Callable[[np.ndarray], bool], noise: bool = True,
-                      device_clock: bool = False) -> N.BandResult:
+                      device_clock: bool = False, split: bool = False) -> N.BandResult:
         """generate_band (src/pipeline.rs:836-1019); `sink(chunk)` returns True to stop.
 
         device_clock=True draws the receiver's white-FM walk on the GPU
@@ -160,7 +160,8 @@ class Prepared:
 
         cb = N.SINK_FN(_sink)
         res = N.BandResult()
-        flags = (N.LPK_NOISE_ON if noise else N.LPK_NOISE_OFF) | (N.LPK_GEN_DEVICE_CLOCK if device_clock else 0)
+        flags = (N.LPK_NOISE_ON if noise else N.LPK_NOISE_OFF) | (N.LPK_GEN_DEVICE_CLOCK if device_clock else 0) \
+            | (N.LPK_GEN_SPLIT if split else 0)
         code = N.lib().lpk_generate_band(self.h, r, b, seed & 0xFFFFFFFFFFFFFFFF, work_idx, max(1, chunk_samples),
                                          flags, cb, None, C.byref(res))
         if err:

@@ -1,0 +1,120 @@
+"""The split-precision fan-out (LPK_SOLVER_SPLIT) against the all-FP64
+reference-semantics kernel and the CPU oracle.
+
+Bars (the target of the split path):
+  * emission delay within 1 ps of the FP64 reference solve;
+  * carrier phase within 1e-6 rad of the FP64 reference phase;
+  * chip / bit / symbol indices bit-exact (a flipped index flips or zeroes a
+    contribution, far outside the IQ tolerance below);
+  * IQ within 1e-5 x max|reference|.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from lipika_b200 import native as N
+from lipika_b200 import pipeline as P
+from oracle import oracle as O
+from tests import scenes
+
+pytestmark = pytest.mark.gpu
+
+DELAY_TOL_S = 1e-12
+PHASE_TOL_RAD = 1e-6
+IQ_RTOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = N.Context(0)
+    yield c
+    c.close()
+
+
+def _contrib(ctx, d, tx, i0, n, solver):
+    d.solver = solver
+    out = (N.CF32 * n)()
+    ph, te, rg = np.zeros(n), np.zeros(n), np.zeros(n)
+    N.check(N.lib().lpk_tx_contribution(ctx.h, C.byref(d), tx, i0, n, None, None, out, N.dptr(ph), N.dptr(te),
+                                        N.dptr(rg)), ctx.h)
+    iq = np.ctypeslib.as_array(C.cast(out, C.POINTER(C.c_float)), (2 * n,)).view(np.complex64).copy()
+    return iq, ph, te, rg / 299792458.0
+
+
+def _check_split_vs_reference(ctx, scene, starts, n, clock_mode=N.LPK_CLOCK_DEVICE_WALK):
+    prep = P.Prepared(scene, ctx)
+    worst = {"delay": 0.0, "phase": 0.0, "iq": 0.0}
+    for (r, b) in prep.work():
+        d = prep.band_desc(r, b, 2026, 0)
+        d.clock_mode = clock_mode
+        for tx in prep.active(r, b):
+            for i0 in starts:
+                i0 = min(i0, max(prep.n_samples(r, b) - n, 0))
+                ref = _contrib(ctx, d, tx, i0, n, N.LPK_SOLVER_REFERENCE)
+                spl = _contrib(ctx, d, tx, i0, n, N.LPK_SOLVER_SPLIT)
+                dd = float(np.max(np.abs(spl[3] - ref[3])))
+                dp = float(np.max(np.abs(np.angle(np.exp(1j * (spl[1] - ref[1]))))))
+                scale = float(np.max(np.abs(ref[0])))
+                di = float(np.max(np.abs(spl[0].astype(np.complex128) - ref[0]))) / max(scale, 1e-30)
+                assert dd <= DELAY_TOL_S, (r, b, tx, i0, dd)
+                assert dp <= PHASE_TOL_RAD, (r, b, tx, i0, dp)
+                assert di <= IQ_RTOL, (r, b, tx, i0, di)
+                worst = {k: max(worst[k], v) for k, v in (("delay", dd), ("phase", dp), ("iq", di))}
+    prep.close()
+    return worst
+
+
+def test_split_matches_reference_dual_band(ctx):
+    w = _check_split_vs_reference(ctx, scenes.config_c1(duration_s=120.0),
+                                  starts=[0, 1_234_567, 100_000_000, 245_000_000], n=300_000)
+    print("split vs FP64 reference, dual-band scene:", w)
+
+
+def test_split_matches_reference_every_signal_kind(ctx):
+    sc = scenes.config_c4(duration_s=60.0, n_rx=2)
+    w = _check_split_vs_reference(ctx, sc, starts=[0, 60_000_000, 122_000_000], n=65_536)
+    print("split vs FP64 reference, 64-transmitter scene:", w)
+
+
+def test_split_handles_anchored_gated_and_deterministic_clock(ctx):
+    sc = scenes.config_c4(duration_s=2.0, n_rx=1)
+    for t in sc.transmitters:
+        if t.kind == "ca_code":
+            t.params["nav"] = "off"
+        t.signal_epoch_unix = 1_000_000_007.25
+    from lipika_b200 import config as cfg
+    sc.transmitters[0].gate = cfg.Gate(0.01, [(0.0, 0.003), (0.005, 0.002)], 3.0)
+    sc.transmitters[20].gate = cfg.Gate(0.007, [(0.001, 0.004)], 0.0)
+    _check_split_vs_reference(ctx, sc, starts=[0, 1_000_000], n=50_000, clock_mode=N.LPK_CLOCK_DETERMINISTIC)
+
+
+def test_split_band_output_matches_oracle(ctx):
+    sc = scenes.config_c1(duration_s=0.1)
+    prep = P.Prepared(sc, ctx)
+    osc = O.Scene(sc)
+    for w, (r, b) in enumerate(prep.work()):
+        parts = []
+        prep.generate_band(r, b, 7, w, 1 << 16, lambda c: parts.append(c) and False, noise=False, split=True)
+        g = np.concatenate(parts)
+        ref = osc.generate_band(r, b, 7, w, 1 << 16, 1, O.NOISE_NONE)["iq"]
+        scale = float(np.max(np.abs(ref)))
+        assert float(np.max(np.abs(g.astype(np.complex128) - ref))) <= IQ_RTOL * scale
+    prep.close()
+
+
+def test_split_chunk_invariant(ctx):
+    sc = scenes.config_c1(duration_s=0.2)
+    prep = P.Prepared(sc, ctx)
+    outs = []
+    for chunk in (1 << 20, 3333):
+        got = []
+        for w, (r, b) in enumerate(prep.work()):
+            parts = []
+            prep.generate_band(r, b, 5, w, chunk, lambda c: parts.append(c) and False, noise=True,
+                               device_clock=True, split=True)
+            got.append(np.concatenate(parts))
+        outs.append(got)
+    for a, b in zip(*outs):
+        assert a.tobytes() == b.tobytes()
+    prep.close()
