@@ -42,8 +42,9 @@ def build(force: bool = False, verbose: bool = False) -> str:
     inc = ["-I" + os.path.join(HERE, "..", "include")]
     for f in CU:
         o = os.path.join(BUILD, f + ".o")
+        extra = os.environ.get("LPK_NVCC_FLAGS", "").split()  # e.g. tile-shape sweeps
         cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
-               "-Xptxas", "-v" if verbose else "-O3", *inc, "-c", os.path.join(CSRC, f), "-o", o]
+               "-Xptxas", "-v" if verbose else "-O3", *extra, *inc, "-c", os.path.join(CSRC, f), "-o", o]
         subprocess.run(cmd, check=True)
         objs.append(o)
     for f in CPP:

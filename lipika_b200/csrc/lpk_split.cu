@@ -133,36 +133,30 @@ k_split_anchor(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__
     recs[id] = r;
 }
 
-// The split-precision contribution of one transmitter at one sample, without
-// branches on the data path. Returns false when the sample needs the exact
-// path (outside the fit, near a rounding tie of the query, or within the
-// guard band of an index boundary); cr/ci are then meaningless.
-__device__ __forceinline__ bool split_sample(const DevTx &tx, const AnchorRec &R, double epoch, double tl,
-                                             double dl, double tu, float &cr, float &ci, double *ph_out,
-                                             double *te_out, double *dl_out) {
-    bool ok = tu >= R.tu0 && tu <= R.tu_hi;
-    const double d = tu - R.tu0;
-    const double t0 = __dsub_rn(tu, kEmissionLag);          // the reference's first query
-    const double s0 = __dadd_rn(epoch, t0);
-    const double q0 = __dsub_rn(__dsub_rn(s0, epoch), t0);  // its rounding offset (exact)
-    const double t1s = tu - poly2(s0 >= R.node0 ? R.p0b : R.p0a, d);
-    const double t1r = fma(-R.k0, q0, t1s);                 // the reference's t1
-    const double s1 = __dadd_rn(epoch, t1r);                 // its second query
-    const double e1 = __dsub_rn(s1, epoch);
-    ok &= fabs(fabs(e1 - t1r) - 0.5 * R.ulp_q) > R.tie;
-    const bool pb = s1 >= R.node1;
-    const double delay = fma(pb ? R.k1b : R.k1a, e1 - t1s, poly2(pb ? R.p1b : R.p1a, d));
-    const double te = tu - delay;
-    float bre = 0.0f, bim = 0.0f;
-    switch (tx.sig_kind) {
-    case kCa: {
+// Per-sample values shared by every transmitter of the band: local and UTC
+// reception times, clock offset, and the first trajectory query (epoch + t0
+// with t0 = tu - 70 ms, the same for every transmitter) with its rounding.
+struct SampleCtx {
+    double tl, dl, q0;  // tu = tl - dl and the query epoch + t0 are recomputed where needed
+};
+
+constexpr int kKindCa = 0, kKindFramed = 1, kKindCw = 2;
+
+// Baseband of one kind at emission time te; clears ok within the guard band
+// of a chip / bit / symbol boundary.
+template <int K>
+__device__ __forceinline__ void split_baseband(const DevTx &tx, const AnchorRec &R, double te, double guard, bool &ok,
+                                               float &bre, float &bim) {
+    bre = 0.0f;
+    bim = 0.0f;
+    if constexpr (K == kKindCa) {
         const double dt = __dsub_rn(te, tx.epoch_rel);
         const double cp = __dmul_rn(dt, kCaChipRate);
-        const double fl = floor(cp), fr = cp - fl, g = R.guard * kCaChipRate;
+        const double fl = floor(cp), fr = cp - fl, g = guard * kCaChipRate;
         ok &= fr >= g && fr <= 1.0 - g && fabs(fl) <= 1.0e9;
         int nav = R.nav_pm;
         if (tx.nav_kind != kNavOff && !(R.flags & kRecNavConst)) {
-            const double nb = __dmul_rn(dt, kNavBitRate), nfl = floor(nb), nfr = nb - nfl, g2 = R.guard * kNavBitRate;
+            const double nb = __dmul_rn(dt, kNavBitRate), nfl = floor(nb), nfr = nb - nfl, g2 = guard * kNavBitRate;
             ok &= nfr >= g2 && nfr <= 1.0 - g2;
             const int64_t bi = (int64_t)nfl;
             if (tx.nav_kind == kNavDummy) nav = nav_bit_pm(tx.nav_seed, bi);
@@ -174,13 +168,9 @@ __device__ __forceinline__ bool split_sample(const DevTx &tx, const AnchorRec &R
         m += m < 0 ? 1023 : 0;
         const int chip = ((tx.chip_neg[m >> 5] >> (m & 31)) & 1u) ? -1 : 1;
         bre = (float)(chip * nav);
-        break;
-    }
-    case kBpsk:
-    case kOok:
-    case kQam16: {
+    } else if constexpr (K == kKindFramed) {
         const double f = __dmul_rn(__dsub_rn(te, tx.epoch_rel), tx.rate);
-        const double fl = floor(f), fr = f - fl, g = R.guard * tx.rate;
+        const double fl = floor(f), fr = f - fl, g = guard * tx.rate;
         ok &= fr >= g && fr <= 1.0 - g;
         const int64_t slot = frame_slot(tx, (int64_t)fl, R.sym_raw0, R.sym_pos0);
         if (slot >= 0) {
@@ -188,35 +178,94 @@ __device__ __forceinline__ bool split_sample(const DevTx &tx, const AnchorRec &R
             else if (tx.sig_kind == kOok) bre = (float)__ldg(tx.ook + slot);
             else { const float2 s = __ldg(tx.sym + slot); bre = s.x; bim = s.y; }
         }
-        break;
-    }
-    default: {  // kCw: the reference rounds ω·t to f32 before an f32 sin/cos (cw.rs:45-50)
+    } else {  // CW: the reference rounds ω·t to f32 before an f32 sin/cos (cw.rs:45-50)
         const float ph = tx.cw_anchored
                              ? (float)f64_rem_euclid(__dadd_rn(__dmul_rn(tx.cw_omega, te), tx.cw_phase0), kTau)
                              : (float)__dmul_rn(tx.cw_omega, te);
         sincosf(ph, &bim, &bre);
-        break;
     }
-    }
-    // carrier phase −2π f (delay + Δt) + 2π (f − f_lo) t_local, reduced mod 2π
-    const double phase = fma(R.tau_if, tl, tx.neg_tau_src * (delay + dl));
-    const double kq = rint(phase * 0.15915494309189535);
-    double rr = fma(-kq, 6.2831854820251465, phase);  // 2π to 24 bits: kq·hi exact
-    rr = fma(-kq, -1.748455600074497e-07, rr);        // 2π − hi
-    const float rf = (float)rr, dr = (float)(rr - (double)rf);
-    float s, c;
-    __sincosf(rf, &s, &c);
-    const float sc = fmaf(dr, c, s), cc = fmaf(-dr, s, c);
-    const float amp = fmaf(R.amp1, (float)d, R.amp0);
-    cr = amp * (bre * cc - bim * sc);
-    ci = amp * (bre * sc + bim * cc);
-    if (ph_out) *ph_out = rr;
-    if (te_out) *te_out = te;
-    if (dl_out) *dl_out = delay;
-    return ok;
 }
 
-__global__ void __launch_bounds__(kSplitThreads)
+// One transmitter over the thread's S samples (the split fast path). A
+// sample outside the fit, within `tie` of a rounding tie of the second
+// query, or within the guard band of an index boundary sets its bit in
+// `redo` and is left to the exact path. DBG stores the diagnostics.
+template <int K, bool DBG, bool KINK, int S>
+__device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, double epoch, const SampleCtx *sc,
+                                           const bool *live, float *ar, float *ai, unsigned &redo, int64_t first,
+                                           double *dbg_phase, double *dbg_temit, double *dbg_delay) {
+    const double tu0 = R.tu0, tu_hi = R.tu_hi, node0 = R.node0, node1 = R.node1, k0 = R.k0, tie = R.tie;
+    const double half = 0.5 * R.ulp_q, tau_if = R.tau_if, nts = tx.neg_tau_src, guard = R.guard;
+    const float amp0 = R.amp0, amp1 = R.amp1;
+    // one piece per iterate (no grid node inside the tile): coefficients in registers
+    const double a0 = R.p0a[0], a1 = R.p0a[1], a2 = R.p0a[2], b0 = R.p1a[0], b1 = R.p1a[1], b2 = R.p1a[2];
+    const double ka = R.k1a;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        if (!live[s]) continue;
+        const SampleCtx &c = sc[s];
+        const double tu = __dsub_rn(c.tl, c.dl);  // src/pipeline.rs:927
+        bool ok = tu >= tu0 && tu <= tu_hi;
+        const double d = tu - tu0;
+        double t1s, poly1, k1;
+        const double *p1 = nullptr;
+        if constexpr (KINK) {
+            const double *p0 = __dadd_rn(epoch, __dsub_rn(tu, kEmissionLag)) >= node0 ? R.p0b : R.p0a;
+            t1s = tu - fma(d, fma(d, p0[2], p0[1]), p0[0]);
+        } else {
+            t1s = tu - fma(d, fma(d, a2, a1), a0);
+        }
+        const double t1r = fma(-k0, c.q0, t1s);  // the reference's t1
+        const double s1 = __dadd_rn(epoch, t1r);  // its second query
+        const double e1 = __dsub_rn(s1, epoch);
+        ok &= fabs(fabs(e1 - t1r) - half) > tie;
+        if constexpr (KINK) {
+            const bool pb = s1 >= node1;
+            p1 = pb ? R.p1b : R.p1a;
+            poly1 = fma(d, fma(d, p1[2], p1[1]), p1[0]);
+            k1 = pb ? R.k1b : R.k1a;
+        } else {
+            poly1 = fma(d, fma(d, b2, b1), b0);
+            k1 = ka;
+        }
+        (void)p1;
+        const double delay = fma(k1, e1 - t1s, poly1);
+        const double te = tu - delay;
+        float bre, bim;
+        split_baseband<K>(tx, R, te, guard, ok, bre, bim);
+        // carrier phase −2π f (delay + Δt) + 2π (f − f_lo) t_local, reduced mod 2π
+        const double phase = fma(tau_if, c.tl, nts * (delay + c.dl));
+        const double kq = rint(phase * 0.15915494309189535);
+        double rr = fma(-kq, 6.2831854820251465, phase);  // 2π to 24 bits: kq·hi exact
+        rr = fma(-kq, -1.748455600074497e-07, rr);        // 2π − hi
+        const float rf = (float)rr, dr = (float)(rr - (double)rf);
+        float sn, cs;
+        __sincosf(rf, &sn, &cs);
+        const float sc2 = fmaf(dr, cs, sn), cc2 = fmaf(-dr, sn, cs);
+        const float amp = fmaf(amp1, (float)d, amp0);
+        if (ok) {
+            ar[s] = fmaf(amp, bre * cc2 - bim * sc2, ar[s]);
+            ai[s] = fmaf(amp, bre * sc2 + bim * cc2, ai[s]);
+        } else {
+            redo |= 1u << s;
+        }
+        if constexpr (DBG) {
+            const int64_t j = first + s * kSplitThreads + threadIdx.x;
+            dbg_phase[j] = rr;
+            dbg_temit[j] = te;
+            dbg_delay[j] = delay;
+        }
+    }
+}
+
+template <bool DBG>
+// At least 3 resident blocks per SM (<= 80 registers): measured on the
+// dual-band scene, occupancy outweighs the few register spills it costs
+// (1 block/SM unconstrained: 5.7e10 tx·rx/s; 3 blocks: 1.05e11).
+#ifndef LPK_SPLIT_MINB
+#define LPK_SPLIT_MINB 3
+#endif
+__global__ void __launch_bounds__(kSplitThreads, LPK_SPLIT_MINB)
 k_band_split(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__restrict__ active, int32_t n_active,
              int64_t t0, const AnchorRec *__restrict__ recs, float2 *__restrict__ out, double *dbg_phase,
              double *dbg_temit, double *dbg_delay) {
@@ -238,8 +287,7 @@ k_band_split(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__re
     }
     __syncthreads();
     constexpr int S = kSplitTile / kSplitThreads;
-    const bool dbg = dbg_phase != nullptr;
-    double tl[S], dl[S], tu[S];
+    SampleCtx sc[S];
     float ar[S], ai[S];
     bool live[S];
 #pragma unroll
@@ -247,46 +295,50 @@ k_band_split(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__re
         const int64_t j = first + s * kSplitThreads + threadIdx.x;
         live[s] = j >= 0 && j < b.n;
         ar[s] = ai[s] = 0.0f;
-        tl[s] = dl[s] = tu[s] = 0.0;
+        sc[s] = SampleCtx{0.0, 0.0, 0.0};
         if (live[s]) {
-            tl[s] = __ddiv_rn((double)(b.i0 + j), b.fs);  // src/pipeline.rs:918
-            dl[s] = band_delta(b, j, tl[s]);
-            tu[s] = __dsub_rn(tl[s], dl[s]);               // :927
+            const double tl = __ddiv_rn((double)(b.i0 + j), b.fs);  // src/pipeline.rs:918
+            const double dl = band_delta(b, j, tl);
+            const double tu = __dsub_rn(tl, dl);                     // :927
+            const double t0q = __dsub_rn(tu, kEmissionLag);
+            const double s0 = __dadd_rn(b.epoch, t0q);
+            sc[s] = SampleCtx{tl, dl, __dsub_rn(__dsub_rn(s0, b.epoch), t0q)};
         }
     }
     for (int k = 0; k < n_active; ++k) {
         const AnchorRec &R = srec[k];
         const bool gate_off = (R.flags & kRecGateOff) != 0;
-        if (gate_off && !dbg) continue;
+        if (gate_off && !DBG) continue;
         const DevTx &T = stx[k];
-        const bool exact_tile = (R.flags & kRecExact) || gate_off;
-        unsigned redo = 0;
-        if (!exact_tile) {
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                const int64_t j = first + s * kSplitThreads + threadIdx.x;
-                float cr, ci;
-                const bool ok = split_sample(T, R, b.epoch, tl[s], dl[s], tu[s], cr, ci,
-                                             dbg && live[s] ? dbg_phase + j : nullptr,
-                                             dbg && live[s] ? dbg_temit + j : nullptr,
-                                             dbg && live[s] ? dbg_delay + j : nullptr);
-                if (ok) { ar[s] += cr; ai[s] += ci; }
-                else redo |= 1u << s;
+        unsigned redo = (1u << S) - 1u;
+        if (!(R.flags & kRecExact) && !gate_off) {
+            redo = 0;
+            const bool kink = R.node0 < kInf || R.node1 < kInf;  // warp-uniform
+#define LPK_PASS(KIND, KNK) \
+    split_pass<KIND, DBG, KNK, S>(T, R, b.epoch, sc, live, ar, ai, redo, first, dbg_phase, dbg_temit, dbg_delay)
+            if (T.sig_kind == kCa) {
+                if (kink) LPK_PASS(kKindCa, true); else LPK_PASS(kKindCa, false);
+            } else if (T.sig_kind == kCw) {
+                if (kink) LPK_PASS(kKindCw, true); else LPK_PASS(kKindCw, false);
+            } else {
+                if (kink) LPK_PASS(kKindFramed, true); else LPK_PASS(kKindFramed, false);
             }
-        } else {
-            redo = (1u << S) - 1u;
+#undef LPK_PASS
         }
+        if (redo == 0) continue;
 #pragma unroll
         for (int s = 0; s < S; ++s) {  // the exact path: rare samples, or whole exact tiles
             if (!((redo >> s) & 1u) || !live[s]) continue;
-            const int64_t j = first + s * kSplitThreads + threadIdx.x;
             float cr = 0.0f, ci = 0.0f;
             double ph = 0.0, te = 0.0, rg = 0.0;
-            contribution(T, b, tl[s], tu[s], dl[s], b.rx[0], b.rx[1], b.rx[2], cr, ci, &ph, &te, &rg);
-            if (!gate_off || dbg) {
-                if (!gate_off) { ar[s] += cr; ai[s] += ci; }
+            contribution(T, b, sc[s].tl, __dsub_rn(sc[s].tl, sc[s].dl), sc[s].dl, b.rx[0], b.rx[1], b.rx[2], cr, ci, &ph, &te, &rg);
+            if (!gate_off) { ar[s] += cr; ai[s] += ci; }
+            if constexpr (DBG) {
+                const int64_t j = first + s * kSplitThreads + threadIdx.x;
+                dbg_phase[j] = ph;
+                dbg_temit[j] = te;
+                dbg_delay[j] = rg * b.inv_c;
             }
-            if (dbg) { dbg_phase[j] = ph; dbg_temit[j] = te; dbg_delay[j] = rg * b.inv_c; }
         }
     }
 #pragma unroll
@@ -318,12 +370,13 @@ cudaError_t launch_band_split(const DevBand &b, const DevTx *d_tx, const int32_t
         if (e != cudaSuccess) return e;
     }
     const size_t smem = (sizeof(DevTx) + sizeof(AnchorRec)) * (size_t)n_active;
+    auto kern = dbg_phase ? k_band_split<true> : k_band_split<false>;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_band_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    k_band_split<<<(unsigned)n_tiles, kSplitThreads, smem, s>>>(b, d_tx, d_active, n_active, t0, recs, d_out,
-                                                                dbg_phase, dbg_temit, dbg_delay);
+    kern<<<(unsigned)n_tiles, kSplitThreads, smem, s>>>(b, d_tx, d_active, n_active, t0, recs, d_out, dbg_phase,
+                                                        dbg_temit, dbg_delay);
     return cudaGetLastError();
 }
 

@@ -26,8 +26,14 @@
 
 namespace lpk {
 
-constexpr int kSplitTile = 1024;      // band samples per anchor tile
-constexpr int kSplitThreads = 256;    // 4 samples per thread
+#ifndef LPK_SPLIT_TILE
+#define LPK_SPLIT_TILE 1024
+#endif
+#ifndef LPK_SPLIT_THREADS
+#define LPK_SPLIT_THREADS 256
+#endif
+constexpr int kSplitTile = LPK_SPLIT_TILE;        // band samples per anchor tile
+constexpr int kSplitThreads = LPK_SPLIT_THREADS;  // kSplitTile / kSplitThreads samples per thread
 // Tiles are aligned to absolute band-sample indices and fitted over a tu range
 // that depends only on the tile and the clock's deterministic trend, widened
 // by kSplitMargin; a sample whose tu falls outside takes the exact path. So
