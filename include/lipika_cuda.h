@@ -229,6 +229,72 @@ lpk_status lpk_clock_device_delta(lpk_ctx *ctx, const lpk_band_desc *band, int64
 lpk_status lpk_rx_chain_apply(lpk_ctx *ctx, const lpk_band_desc *band, lpk_cf32 *iq, int64_t n);
 
 /* ------------------------------------------------------------------ */
+/* Launch shapes of the split-precision fan-out                        */
+/* ------------------------------------------------------------------ */
+/* The split kernel is compiled in several launch shapes (band samples per
+ * tile, threads per block, minimum resident blocks per SM). No reference
+ * counterpart: the reference has one CPU loop. */
+int32_t lpk_split_variant_count(void);
+lpk_status lpk_split_variant_info(int32_t variant, int32_t *tile, int32_t *threads, int32_t *min_blocks);
+/* Shape used by this context's single-band entry points (default 0). */
+lpk_status lpk_ctx_set_split_variant(lpk_ctx *ctx, int32_t variant);
+int32_t lpk_ctx_split_variant(const lpk_ctx *ctx);
+
+/* ------------------------------------------------------------------ */
+/* Batched fan-out: every (receiver, band) work unit in one launch     */
+/* ------------------------------------------------------------------ */
+/* Replaces the per-work-unit loop of run_scene_to_dir / run_scene_in_memory
+ * (src/pipeline.rs:460-536: one generate_band per (rx, band), run by rayon
+ * workers) for a whole scene at once. Time advances in rounds of round_s
+ * seconds: in round k unit u renders band samples [k L_u, (k+1) L_u) with
+ * L_u = llround(round_s * fs_u), clipped to its length, so units of uneven
+ * rate and length progress together. One round is one CUDA graph (a copy of
+ * the round's descriptor, the clock walks of every receiver, the anchor
+ * fits of every (unit, tile, transmitter), and one persistent fan-out kernel
+ * that pulls tiles of every unit from a shared counter); the graph is built
+ * once and replayed. Outputs equal the single-band entry points' for the
+ * same solver and split launch shape (chunk invariance).
+ * Units need a stationary receiver (rx_kind LPK_RX_STATIONARY) and a clock
+ * mode of LPK_CLOCK_DETERMINISTIC or LPK_CLOCK_DEVICE_WALK; units whose
+ * clock seed, master rate and Allan deviation agree share one walk (the
+ * bands of one receiver). Units with solver LPK_SOLVER_REFERENCE or an
+ * antenna take the reference-exact path for every sample. */
+typedef struct lpk_batch lpk_batch;
+typedef struct lpk_work_unit {
+    lpk_band_desc band;
+    const int32_t *active;   /* in-band transmitters, summed in this order (host memory) */
+    int32_t n_active;
+    int32_t reserved;
+    int64_t n_samples;       /* band length */
+} lpk_work_unit;
+
+lpk_status lpk_batch_create(lpk_ctx *ctx, const lpk_work_unit *units, int32_t n_units, double round_s,
+                            lpk_batch **out);
+void lpk_batch_destroy(lpk_batch *b);
+int64_t lpk_batch_n_rounds(const lpk_batch *b);
+/* Band samples [*i0, *i0 + *n) of unit `unit` in round `round`. */
+lpk_status lpk_batch_round_extent(const lpk_batch *b, int64_t round, int32_t unit, int64_t *i0, int64_t *n);
+/* Enqueue round `round` on the context's stream (asynchronous). Rounds may
+ * run in any order; the walk carries they need are completed on the way. */
+lpk_status lpk_batch_run(lpk_batch *b, int64_t round);
+/* Device pointer of unit `unit`'s output of the last round run (valid until
+ * the next lpk_batch_run). */
+lpk_status lpk_batch_output(lpk_batch *b, int32_t unit, const lpk_cf32 **d_out);
+/* Wait for the last round and copy unit `unit`'s output to host memory. */
+lpk_status lpk_batch_copy_out(lpk_batch *b, int32_t unit, lpk_cf32 *host, int64_t cap);
+/* Launch configuration: split shape and persistent blocks per SM (0 = the
+ * most that fit). */
+lpk_status lpk_batch_set_config(lpk_batch *b, int32_t variant, int32_t blocks_per_sm);
+lpk_status lpk_batch_get_config(const lpk_batch *b, int32_t *variant, int32_t *blocks_per_sm,
+                                int32_t *max_blocks_per_sm);
+/* Autotuner: run round `round` under every (variant, blocks per SM) pair
+ * the device can hold (blocks per SM: the maximum, and half of it),
+ * `reps` timed replays each after one warm-up, keep the fastest. ms_table
+ * (may be NULL) receives lpk_split_variant_count() x 2 mean milliseconds
+ * per round (negative where a pair was skipped). */
+lpk_status lpk_batch_autotune(lpk_batch *b, int64_t round, int32_t reps, double *ms_table);
+
+/* ------------------------------------------------------------------ */
 /* Host-level mirror of src/pipeline.rs (scene -> per-band streams)     */
 /* ------------------------------------------------------------------ */
 typedef struct lpk_scene lpk_scene;
@@ -289,6 +355,18 @@ lpk_status lpk_generate_band(lpk_scene *s, int32_t r_idx, int32_t b_idx, uint64_
 lpk_status lpk_generate_band_to_file(lpk_scene *s, int32_t r_idx, int32_t b_idx, uint64_t seed_base,
                                      int32_t work_idx, int64_t chunk_samples, int32_t flags,
                                      const char *path, lpk_band_result *result);
+
+/* Every work unit of the scene through one lpk_batch (run_scene_in_memory /
+ * run_scene_to_dir, src/pipeline.rs:460-536, with the per-unit
+ * generate_band calls fused): rounds of round_s seconds, each unit's chunk
+ * handed to sink_unit(user, work_idx, chunk, n) in order. Work units whose
+ * receiver moves or whose clock has flicker are rendered by
+ * lpk_generate_band instead, after the batch. Flags as lpk_generate_band,
+ * plus LPK_GEN_AUTOTUNE (tune the launch shape on the middle round first). */
+enum { LPK_GEN_AUTOTUNE = 8 };
+typedef int32_t (*lpk_unit_sink_fn)(void *user, int32_t work_idx, const lpk_cf32 *chunk, int64_t n);
+lpk_status lpk_generate_scene(lpk_scene *s, uint64_t seed_base, double round_s, int32_t flags,
+                              lpk_unit_sink_fn sink, void *user);
 
 /* Host clock stream (ClockStream, src/clock/mod.rs:229-347) exposed for
  * tests: delta_t_at over n monotone times. */

@@ -512,7 +512,7 @@ lpk_status lpk_band_chunk_device(lpk_ctx *c, const lpk_band_desc *band, const in
     int64_t kA = 0, span = b.clock_mode == LPK_CLOCK_DEVICE_WALK ? walk_span(band, i0, n, &kA) : 0;
     const bool split = use_split(band);
     size_t off_recs = off_eps + align256(sizeof(double) * (size_t)span);
-    size_t recs = split ? align256(split_recs_bytes(i0, n, n_active)) : 0;
+    size_t recs = split ? align256(split_recs_bytes(c->split_variant, i0, n, n_active)) : 0;
     if ((st = ensure_scratch(c, off_recs + recs))) return st;
     int32_t *d_active = (int32_t *)c->d_scratch;
     uint32_t *d_uw = (uint32_t *)((char *)c->d_scratch + off_uw);
@@ -523,7 +523,7 @@ lpk_status lpk_band_chunk_device(lpk_ctx *c, const lpk_band_desc *band, const in
     if (span && (st = prepare_walk(c, band, i0, n, b, (double *)((char *)c->d_scratch + off_eps), span))) return st;
     prof_begin(c);
     if (split)
-        e = launch_band_split(b, c->d_tx, d_active, n_active, (char *)c->d_scratch + off_recs, (float2 *)d_out,
+        e = launch_band_split(c->split_variant, b, c->d_tx, d_active, n_active, (char *)c->d_scratch + off_recs, (float2 *)d_out,
                               nullptr, nullptr, nullptr, c->stream);
     else
         e = launch_band_reference(b, c->d_tx, d_active, n_active, (float2 *)d_out, d_uw, c->stream);
@@ -568,7 +568,7 @@ lpk_status lpk_band_chunk(lpk_ctx *c, const lpk_band_desc *band, const int32_t *
     int64_t kA = 0, span = b.clock_mode == LPK_CLOCK_DEVICE_WALK ? walk_span(band, i0, n, &kA) : 0;
     const bool split = use_split(band);
     size_t off_recs = off_eps + align256(sizeof(double) * (size_t)span);
-    size_t total = off_recs + (split ? align256(split_recs_bytes(i0, n, n_active)) : 0);
+    size_t total = off_recs + (split ? align256(split_recs_bytes(c->split_variant, i0, n, n_active)) : 0);
     if ((st = ensure_scratch(c, total))) return st;
     char *base = (char *)c->d_scratch;
     int32_t *d_active = (int32_t *)(base + off_active);
@@ -589,7 +589,7 @@ lpk_status lpk_band_chunk(lpk_ctx *c, const lpk_band_desc *band, const int32_t *
     if (span && (st = prepare_walk(c, band, i0, n, b, (double *)(base + off_eps), span))) return st;
     prof_begin(c);
     if (split)
-        e = launch_band_split(b, c->d_tx, d_active, n_active, base + off_recs, d_out, nullptr, nullptr, nullptr,
+        e = launch_band_split(c->split_variant, b, c->d_tx, d_active, n_active, base + off_recs, d_out, nullptr, nullptr, nullptr,
                               c->stream);
     else
         e = launch_band_reference(b, c->d_tx, d_active, n_active, d_out, d_uw, c->stream);
@@ -651,7 +651,7 @@ lpk_status lpk_tx_contribution(lpk_ctx *c, const lpk_band_desc *band, int32_t tx
     size_t off_act = 8 * bytes;
     size_t off_eps = off_act + 256;
     size_t off_recs = off_eps + align256(sizeof(double) * (size_t)span);
-    lpk_status s2 = ensure_scratch(c, off_recs + (split ? align256(split_recs_bytes(i0, n, 1)) : 0) + 256);
+    lpk_status s2 = ensure_scratch(c, off_recs + (split ? align256(split_recs_bytes(c->split_variant, i0, n, 1)) : 0) + 256);
     if (s2) return s2;
     double *d_delta = (double *)c->d_scratch;
     double *d_rx = d_delta + n;
@@ -672,7 +672,7 @@ lpk_status lpk_tx_contribution(lpk_ctx *c, const lpk_band_desc *band, int32_t tx
     if (split) {
         b.has_noise = 0;  // the contribution alone, as transmitter_contribution_at_receiver returns it
         b.n_post = 0;
-        e = launch_band_split(b, c->d_tx, (const int32_t *)(base + off_act), 1, base + off_recs, d_out, d_phase, d_te,
+        e = launch_band_split(c->split_variant, b, c->d_tx, (const int32_t *)(base + off_act), 1, base + off_recs, d_out, d_phase, d_te,
                               d_r, c->stream);
     } else {
         e = launch_tx_contribution(b, c->d_tx, tx, d_out, d_phase, d_te, d_r, c->stream);

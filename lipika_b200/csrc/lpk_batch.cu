@@ -1,0 +1,709 @@
+// lpk_batch.cu — every (receiver, band) work unit of a scene in one
+// persistent fan-out per round, replayed as a CUDA graph.
+//
+// The reference renders each work unit with its own generate_band call
+// (src/pipeline.rs:506-535, one rayon task per (rx, band)); each call
+// regenerates its receiver's clock walk (src/pipeline.rs:864-873). Here a
+// round advances every unit by the same stretch of time: one graph copies
+// the round's descriptor, scans the clock walk of every receiver once (all
+// bands of a receiver read it), fits the anchors of every (unit, tile,
+// transmitter), and runs one persistent kernel whose blocks pull tiles of
+// all units from a shared counter, so units of uneven rate, length and
+// transmitter count keep every SM busy until the round's last tile.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "lpk_internal.h"
+#include "lpk_split.cuh"
+
+namespace lpk {
+
+namespace {
+
+constexpr int kMaxUnits = 256;
+constexpr int kMaxWalks = kMaxUnits;  // at most one walk per unit
+
+// Per unit, fixed for the batch.
+struct BatchUnit {
+    int32_t act_off, n_active;
+    int32_t walk;        // index into the walk table, -1 without a device walk
+    int32_t exact_only;  // reference-exact path for every sample
+    float2 *out;         // round output buffer (capacity: the unit's round length)
+};
+
+// One receiver clock walk: the scan blocks' totals and carries over the
+// whole scene, and the in-block prefixes of the current round.
+struct DevWalk {
+    uint64_t seed;
+    double sigma;
+    double *partial;  // P_b(k) for k in [bA·kWalkBlock, (bB+1)·kWalkBlock)
+    double *totals;   // per scan block
+    double *carry;    // carry[b] = Σ totals[0..b-1]
+};
+
+// Per round (copied to the device by the graph's first node).
+struct RoundUnit {
+    int64_t i0, n;          // band samples [i0, i0 + n)
+    int64_t t0, n_tiles;    // absolute index of the first tile, tile count
+    int64_t tile_off, rec_off;  // prefix over schedule slots
+    int32_t unit, pad;
+};
+struct RoundWalk {
+    int64_t b_lo, bA, bB;   // blocks [b_lo, bB] are scanned, P_b stored for [bA, bB]
+    int64_t carry_from;     // carries [carry_from + 1, bB] are added
+};
+struct RoundDesc {
+    int64_t total_tiles, total_recs, total_walk_blocks;
+    int32_t n_slots, n_walks, tile, pad;
+    int64_t wb_off[kMaxWalks + 1];  // prefix of scanned blocks per walk
+    RoundWalk w[kMaxWalks];
+    RoundUnit s[kMaxUnits];         // schedule slots, most work first
+};
+
+__device__ __forceinline__ int find_slot_tiles(const RoundDesc &rd, int64_t g) {
+    int lo = 0, hi = rd.n_slots - 1;
+    while (lo < hi) {  // last slot with tile_off <= g
+        int mid = (lo + hi + 1) >> 1;
+        if (rd.s[mid].tile_off <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int find_slot_recs(const RoundDesc &rd, int64_t g) {
+    int lo = 0, hi = rd.n_slots - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (rd.s[mid].rec_off <= g) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Scan blocks of every walk of the round (grid-stride, one block per scan
+// block): totals always, in-block prefixes for [bA, bB].
+__global__ void __launch_bounds__(kWalkThreads)
+k_batch_walk(const DevWalk *__restrict__ walks, const RoundDesc *__restrict__ rd) {
+    __shared__ double warp_tot[kWalkThreads / 32];
+    const int64_t total = rd->total_walk_blocks;
+    for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
+        int w = 0;
+        while (w + 1 < rd->n_walks && rd->wb_off[w + 1] <= g) ++w;
+        const RoundWalk rw = rd->w[w];
+        const DevWalk dw = walks[w];
+        const int64_t b = rw.b_lo + (g - rd->wb_off[w]);
+        double v[kWalkPer], offset;
+        walk_block_prefix(dw.seed, dw.sigma, b, warp_tot, v, offset);
+        if (threadIdx.x == kWalkThreads - 1) dw.totals[b] = __dadd_rn(offset, v[kWalkPer - 1]);
+        if (b >= rw.bA) {
+            const int64_t base = b * kWalkBlock + (int64_t)threadIdx.x * kWalkPer - rw.bA * kWalkBlock;
+#pragma unroll
+            for (int i = 0; i < kWalkPer; ++i) dw.partial[base + i] = __dadd_rn(offset, v[i]);
+        }
+    }
+}
+
+// carry(b + 1) = carry(b) ⊕ total(b) in block order, one warp (block) per
+// walk: 32 totals are loaded at once, the sum stays sequential.
+__global__ void __launch_bounds__(32) k_batch_carry(const DevWalk *__restrict__ walks,
+                                                    const RoundDesc *__restrict__ rd) {
+    const int w = (int)blockIdx.x, lane = (int)threadIdx.x;
+    if (w >= rd->n_walks) return;
+    const RoundWalk rw = rd->w[w];
+    const DevWalk dw = walks[w];
+    double c = dw.carry[rw.carry_from];
+    for (int64_t b0 = rw.carry_from; b0 < rw.bB; b0 += 32) {
+        const int64_t nb = rw.bB - b0 < 32 ? rw.bB - b0 : 32;
+        const double t = lane < nb ? dw.totals[b0 + lane] : 0.0;
+        double mine = 0.0;
+        for (int j = 0; j < (int)nb; ++j) {
+            c = __dadd_rn(c, __shfl_sync(0xffffffffu, t, j));
+            if (lane == j) mine = c;
+        }
+        if (lane < nb) dw.carry[b0 + lane + 1] = mine;
+    }
+}
+
+// Anchor fits of every (slot, tile, transmitter) of the round.
+__global__ void __launch_bounds__(128)
+k_batch_anchor(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ units,
+               const DevTx *__restrict__ txs, const int32_t *__restrict__ act, const RoundDesc *__restrict__ rd,
+               AnchorRec *__restrict__ recs) {
+    const int64_t total = rd->total_recs;
+    const int tile_len = rd->tile;
+    for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < total;
+         id += (int64_t)gridDim.x * blockDim.x) {
+        const int sl = find_slot_recs(*rd, id);
+        const RoundUnit &ru = rd->s[sl];
+        const BatchUnit bu = units[ru.unit];
+        const int64_t local = id - ru.rec_off;
+        const int64_t tile = local / bu.n_active;
+        const int k = (int)(local - tile * bu.n_active);
+        const int64_t gs = (ru.t0 + tile) * tile_len;
+        AnchorRec r;
+        fit_anchor(bands[ru.unit], txs[act[bu.act_off + k]], gs, gs + tile_len - 1, bu.exact_only != 0, r);
+        recs[id] = r;
+    }
+}
+
+// The persistent fan-out: blocks take tiles from the round's counter until
+// none is left. A block restages the band and its transmitters only when
+// the next tile belongs to another unit.
+template <int TILE, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
+k_batch_fanout(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ units,
+               const DevTx *__restrict__ txs, const int32_t *__restrict__ act, const DevWalk *__restrict__ walks,
+               const RoundDesc *__restrict__ rd, const AnchorRec *__restrict__ recs,
+               unsigned long long *__restrict__ counter, int32_t max_active) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    DevBand *sb = reinterpret_cast<DevBand *>(smem_raw);
+    DevTx *stx = reinterpret_cast<DevTx *>(smem_raw + ((sizeof(DevBand) + 15) / 16) * 16);
+    AnchorRec *srec = reinterpret_cast<AnchorRec *>(reinterpret_cast<unsigned char *>(stx) +
+                                                    sizeof(DevTx) * (size_t)max_active);
+    __shared__ unsigned long long s_next;
+    int cur = -1;
+    const int64_t total = rd->total_tiles;
+    for (;;) {
+        if (threadIdx.x == 0) s_next = atomicAdd(counter, 1ull);
+        __syncthreads();
+        const int64_t g = (int64_t)s_next;
+        if (g >= total) break;
+        const int sl = find_slot_tiles(*rd, g);
+        const RoundUnit &ru = rd->s[sl];
+        const BatchUnit bu = units[ru.unit];
+        const int64_t local = g - ru.tile_off;
+        const bool fresh = ru.unit != cur;
+        if (fresh && threadIdx.x == 0) {
+            DevBand b = bands[ru.unit];
+            b.i0 = ru.i0;
+            b.n = ru.n;
+            if (bu.walk >= 0) {
+                b.eps = walks[bu.walk].partial;
+                b.eps_carry = walks[bu.walk].carry;
+                b.eps_k0 = rd->w[bu.walk].bA * kWalkBlock;
+            }
+            *sb = b;
+        }
+        stage_tile(txs, act + bu.act_off, bu.n_active, recs + ru.rec_off + local * bu.n_active, stx, srec, fresh);
+        cur = ru.unit;
+        __syncthreads();
+        const int64_t first = (ru.t0 + local) * TILE - ru.i0;
+        split_tile<TILE / THREADS, THREADS, false>(*sb, stx, srec, bu.n_active, first, bu.out, nullptr, nullptr,
+                                                   nullptr);
+        __syncthreads();  // the next stage overwrites the shared tiles
+    }
+}
+
+using FanoutKernel = void (*)(const DevBand *, const BatchUnit *, const DevTx *, const int32_t *, const DevWalk *,
+                              const RoundDesc *, const AnchorRec *, unsigned long long *, int32_t);
+
+struct FanoutShape {
+    int tile, threads;
+    FanoutKernel kern;
+};
+#define LPK_BATCH_ENTRY(I, T, N, M) {T, N, k_batch_fanout<T, N, M>},
+const FanoutShape kFanout[kSplitVariants] = {LPK_SPLIT_VARIANTS(LPK_BATCH_ENTRY)};
+#undef LPK_BATCH_ENTRY
+
+inline size_t fanout_smem(int max_active) {
+    return ((sizeof(DevBand) + 15) / 16) * 16 + (sizeof(DevTx) + sizeof(AnchorRec)) * (size_t)max_active;
+}
+
+}  // namespace
+}  // namespace lpk
+
+using namespace lpk;
+
+struct UnitHost {
+    lpk_band_desc desc;
+    int64_t n_samples = 0, round_len = 0;
+    int32_t n_active = 0, walk = -1;
+    bool exact_only = false;
+};
+
+struct WalkHost {
+    uint64_t seed = 0;
+    double fm = 0.0, sigma = 0.0;
+    int64_t carry_done = 0;  // carry[b] is known for b <= carry_done
+    int64_t partial_cap = 0;
+};
+
+struct lpk_batch {
+    lpk_ctx *ctx = nullptr;
+    std::vector<UnitHost> units;
+    std::vector<WalkHost> walks;
+    std::vector<void *> allocs;
+    DevBand *d_bands = nullptr;
+    BatchUnit *d_units = nullptr;
+    std::vector<BatchUnit> h_units;
+    int32_t *d_act = nullptr;
+    DevWalk *d_walks = nullptr;
+    RoundDesc *d_round = nullptr;
+    RoundDesc *h_round[2] = {nullptr, nullptr};  // pinned, alternating between rounds
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    AnchorRec *d_recs = nullptr;
+    unsigned long long *d_counter = nullptr;
+    int64_t recs_cap = 0;
+    int64_t n_rounds = 0;
+    int32_t max_active = 0;
+    int variant = 0, bps = 0, max_bps = 0, walk_grid = 0, anchor_grid = 0;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int parity = 0;
+    int64_t last_round = -1;
+};
+
+namespace {
+
+lpk_status batch_alloc(lpk_batch *b, void **p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+    if (e != cudaSuccess) return fail(b->ctx, LPK_ENOMEM, std::string("batch allocation failed: ") +
+                                                                cudaGetErrorString(e));
+    b->allocs.push_back(*p);
+    return LPK_OK;
+}
+
+void unit_extent(const lpk_batch *b, int64_t round, int u, int64_t &i0, int64_t &n) {
+    const UnitHost &uh = b->units[u];
+    i0 = round * uh.round_len;
+    n = uh.n_samples - i0;
+    n = n < 0 ? 0 : (n > uh.round_len ? uh.round_len : n);
+}
+
+// Fill the round descriptor: schedule slots (most work first), tile and
+// anchor prefixes for tile length `tile`, and the walk block ranges. With
+// commit, the walks' carry bookkeeping advances.
+void plan_round(lpk_batch *b, int64_t round, int tile, RoundDesc &rd, bool commit, int64_t *recs_out,
+                int64_t *partial_blocks_out) {
+    memset(&rd, 0, offsetof(RoundDesc, s));
+    rd.tile = tile;
+    std::vector<int> order;
+    for (int u = 0; u < (int)b->units.size(); ++u) {
+        int64_t i0, n;
+        unit_extent(b, round, u, i0, n);
+        if (n > 0) order.push_back(u);
+    }
+    auto cost = [&](int u) {
+        int64_t i0, n;
+        unit_extent(b, round, u, i0, n);
+        return (double)n * (double)(b->units[u].n_active + 1);
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(x) > cost(y); });
+    int64_t tiles = 0, recs = 0;
+    std::vector<int64_t> kA(b->walks.size(), INT64_MAX), kB(b->walks.size(), -1);
+    for (size_t sl = 0; sl < order.size(); ++sl) {
+        const int u = order[sl];
+        const UnitHost &uh = b->units[u];
+        RoundUnit &ru = rd.s[sl];
+        unit_extent(b, round, u, ru.i0, ru.n);
+        ru.t0 = ru.i0 / tile;
+        ru.n_tiles = (ru.i0 + ru.n - 1) / tile - ru.t0 + 1;
+        ru.tile_off = tiles;
+        ru.rec_off = recs;
+        ru.unit = u;
+        tiles += ru.n_tiles;
+        recs += ru.n_tiles * uh.n_active;
+        if (uh.walk >= 0) {
+            int64_t a;
+            int64_t span = walk_span(&uh.desc, ru.i0, ru.n, &a);
+            kA[uh.walk] = std::min(kA[uh.walk], a);
+            kB[uh.walk] = std::max(kB[uh.walk], a + span - 1);
+        }
+    }
+    rd.n_slots = (int32_t)order.size();
+    rd.total_tiles = tiles;
+    rd.total_recs = recs;
+    rd.n_walks = (int32_t)b->walks.size();
+    int64_t wb = 0, partial_blocks = 0;
+    for (size_t w = 0; w < b->walks.size(); ++w) {
+        RoundWalk &rw = rd.w[w];
+        WalkHost &wh = b->walks[w];
+        rd.wb_off[w] = wb;
+        if (kB[w] < 0) {  // no unit of this walk renders in this round
+            rw.b_lo = rw.bA = 0;
+            rw.bB = -1;
+            rw.carry_from = 0;
+            continue;
+        }
+        rw.bA = kA[w] / kWalkBlock;
+        rw.bB = kB[w] / kWalkBlock;
+        rw.b_lo = std::min(rw.bA, wh.carry_done);
+        rw.carry_from = wh.carry_done;
+        if (rw.carry_from > rw.bB) rw.carry_from = rw.bB;  // nothing new to carry
+        wb += rw.bB - rw.b_lo + 1;
+        partial_blocks = std::max(partial_blocks, rw.bB - rw.bA + 1);
+        if (commit) wh.carry_done = std::max(wh.carry_done, rw.bB);
+    }
+    rd.wb_off[b->walks.size()] = wb;
+    rd.total_walk_blocks = wb;
+    if (recs_out) *recs_out = recs;
+    if (partial_blocks_out) *partial_blocks_out = partial_blocks;
+}
+
+void drop_graphs(lpk_batch *b) {
+    for (auto &g : b->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+// Capture the round graph (descriptor copy from h_round[p], walk scan,
+// carries, anchors, counter reset, persistent fan-out) for the current
+// launch configuration.
+lpk_status build_graph(lpk_batch *b, int p) {
+    lpk_ctx *c = b->ctx;
+    const FanoutShape &sh = kFanout[b->variant];
+    const size_t smem = fanout_smem(b->max_active);
+    cudaError_t e = cudaFuncSetAttribute(sh.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(c, e, "batch fan-out shared memory");
+    int dev_sms = 0;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_fail(c, e, "batch graph capture");
+    cudaMemcpyAsync(b->d_round, b->h_round[p], sizeof(RoundDesc), cudaMemcpyHostToDevice, c->stream);
+    if (!b->walks.empty()) {
+        k_batch_walk<<<b->walk_grid, kWalkThreads, 0, c->stream>>>(b->d_walks, b->d_round);
+        k_batch_carry<<<(unsigned)b->walks.size(), 32, 0, c->stream>>>(b->d_walks, b->d_round);
+    }
+    k_batch_anchor<<<b->anchor_grid, 128, 0, c->stream>>>(b->d_bands, b->d_units, c->d_tx, b->d_act, b->d_round,
+                                                          b->d_recs);
+    cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), c->stream);
+    sh.kern<<<(unsigned)(dev_sms * b->bps), sh.threads, smem, c->stream>>>(
+        b->d_bands, b->d_units, c->d_tx, b->d_act, b->d_walks, b->d_round, b->d_recs, b->d_counter, b->max_active);
+    cudaError_t le = cudaGetLastError();
+    e = cudaStreamEndCapture(c->stream, &g);
+    if (le != cudaSuccess || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return cuda_fail(c, le != cudaSuccess ? le : e, "batch graph capture");
+    }
+    e = cudaGraphInstantiate(&b->graph[p], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        b->graph[p] = nullptr;
+        return cuda_fail(c, e, "batch graph instantiate");
+    }
+    return LPK_OK;
+}
+
+lpk_status configure(lpk_batch *b, int variant, int bps) {
+    if (variant < 0 || variant >= kSplitVariants) return fail(b->ctx, LPK_EINVAL, "unknown split variant");
+    const FanoutShape &sh = kFanout[variant];
+    const size_t smem = fanout_smem(b->max_active);
+    cudaError_t e = cudaFuncSetAttribute(sh.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(b->ctx, e, "batch fan-out shared memory");
+    int occ = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sh.kern, sh.threads, smem);
+    if (e != cudaSuccess) return cuda_fail(b->ctx, e, "batch occupancy query");
+    if (occ < 1) return fail(b->ctx, LPK_EINVAL, "batch fan-out does not fit on an SM");
+    if (bps < 0) return fail(b->ctx, LPK_EINVAL, "blocks per SM must be >= 0");
+    drop_graphs(b);
+    b->variant = variant;
+    b->max_bps = occ;
+    b->bps = (bps == 0 || bps > occ) ? occ : bps;
+    return LPK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t lpk_split_variant_count(void) { return kSplitVariants; }
+
+lpk_status lpk_split_variant_info(int32_t v, int32_t *tile, int32_t *threads, int32_t *min_blocks) {
+    int t = 0, n = 0, m = 0;
+    if (!split_variant_info(v, &t, &n, &m)) return fail(nullptr, LPK_EINVAL, "unknown split variant");
+    if (tile) *tile = t;
+    if (threads) *threads = n;
+    if (min_blocks) *min_blocks = m;
+    return LPK_OK;
+}
+
+lpk_status lpk_ctx_set_split_variant(lpk_ctx *c, int32_t v) {
+    if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
+    if (v < 0 || v >= kSplitVariants) return fail(c, LPK_EINVAL, "unknown split variant");
+    c->split_variant = v;
+    return LPK_OK;
+}
+
+int32_t lpk_ctx_split_variant(const lpk_ctx *c) { return c ? c->split_variant : -1; }
+
+void lpk_batch_destroy(lpk_batch *b) {
+    if (!b) return;
+    if (b->ctx) {
+        cudaSetDevice(b->ctx->device);
+        cudaStreamSynchronize(b->ctx->stream);
+    }
+    drop_graphs(b);
+    for (void *p : b->allocs) cudaFree(p);
+    for (auto &h : b->h_round)
+        if (h) cudaFreeHost(h);
+    for (auto &ev : b->done)
+        if (ev) cudaEventDestroy(ev);
+    delete b;
+}
+
+lpk_status lpk_batch_create(lpk_ctx *c, const lpk_work_unit *wu, int32_t n_units, double round_s, lpk_batch **out) {
+    if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
+    if (!out) return fail(c, LPK_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (n_units < 1 || n_units > kMaxUnits) return fail(c, LPK_EINVAL, "batch needs 1..256 work units");
+    if (!wu) return fail(c, LPK_EINVAL, "units is NULL");
+    if (!(round_s > 0.0) || !std::isfinite(round_s)) return fail(c, LPK_EINVAL, "round_s must be positive");
+    cudaSetDevice(c->device);
+    lpk_batch *b = new lpk_batch();
+    b->ctx = c;
+    std::vector<DevBand> h_bands((size_t)n_units);
+    std::vector<int32_t> h_act;
+    lpk_status st = LPK_OK;
+    for (int u = 0; u < n_units && !st; ++u) {
+        const lpk_work_unit &w = wu[u];
+        UnitHost uh;
+        uh.desc = w.band;
+        uh.n_samples = w.n_samples;
+        uh.n_active = w.n_active;
+        if (w.n_samples < 0) st = fail(c, LPK_EINVAL, "work unit length must be >= 0");
+        else if (w.band.rx_kind != LPK_RX_STATIONARY) st = fail(c, LPK_ENOTSUP, "batch units need a stationary receiver");
+        else if (w.band.clock_mode != LPK_CLOCK_DETERMINISTIC && w.band.clock_mode != LPK_CLOCK_DEVICE_WALK)
+            st = fail(c, LPK_ENOTSUP, "batch units need a deterministic or device-walk clock");
+        else if ((st = build_dev_band(c, &w.band, 0, w.n_samples, h_bands[u]))) {
+        } else if ((st = check_active(c, w.active, w.n_active))) {
+        }
+        if (st) break;
+        uh.round_len = std::max<int64_t>(1, std::llround(round_s * w.band.fs_hz));
+        uh.exact_only = !(w.band.solver == LPK_SOLVER_SPLIT) || w.band.has_antenna;
+        if (w.band.clock_mode == LPK_CLOCK_DEVICE_WALK) {
+            const double sigma = w.band.clock_allan_1s / std::sqrt(w.band.clock_master_rate_hz);
+            int found = -1;
+            for (size_t k = 0; k < b->walks.size(); ++k)
+                if (b->walks[k].seed == w.band.clock_seed && b->walks[k].fm == w.band.clock_master_rate_hz &&
+                    b->walks[k].sigma == sigma)
+                    found = (int)k;
+            if (found < 0) {
+                WalkHost wh;
+                wh.seed = w.band.clock_seed;
+                wh.fm = w.band.clock_master_rate_hz;
+                wh.sigma = sigma;
+                b->walks.push_back(wh);
+                found = (int)b->walks.size() - 1;
+            }
+            uh.walk = found;
+            h_bands[u].fm = w.band.clock_master_rate_hz;
+        }
+        BatchUnit bu{};
+        bu.act_off = (int32_t)h_act.size();
+        bu.n_active = w.n_active;
+        bu.walk = uh.walk;
+        bu.exact_only = uh.exact_only;
+        for (int k = 0; k < w.n_active; ++k) h_act.push_back(w.active[k]);
+        b->max_active = std::max(b->max_active, w.n_active);
+        b->units.push_back(uh);
+        b->h_units.push_back(bu);
+    }
+    if (st) {
+        lpk_batch_destroy(b);
+        return st;
+    }
+    for (auto &uh : b->units) {
+        int64_t r = (uh.n_samples + uh.round_len - 1) / uh.round_len;
+        b->n_rounds = std::max(b->n_rounds, r);
+    }
+    // capacities: anchors at the smallest tile, walk prefixes, scene-long carries
+    RoundDesc *tmp = new RoundDesc();
+    std::vector<WalkHost> saved = b->walks;
+    for (int64_t r = 0; r < b->n_rounds; ++r) {
+        int64_t recs = 0, pb = 0;
+        plan_round(b, r, kSplitMinTile, *tmp, true, &recs, &pb);
+        b->recs_cap = std::max(b->recs_cap, recs);
+        for (auto &wh : b->walks) wh.partial_cap = std::max(wh.partial_cap, pb * kWalkBlock);
+    }
+    std::vector<int64_t> total_blocks(b->walks.size(), 1);
+    for (size_t w = 0; w < b->walks.size(); ++w) {
+        total_blocks[w] = b->walks[w].carry_done + 2;
+        saved[w].partial_cap = b->walks[w].partial_cap;
+    }
+    b->walks = saved;  // carry bookkeeping restarts at block 0
+    delete tmp;
+    void *p = nullptr;
+    if (!st) st = batch_alloc(b, &p, sizeof(DevBand) * (size_t)n_units), b->d_bands = (DevBand *)p;
+    if (!st) st = batch_alloc(b, &p, sizeof(BatchUnit) * (size_t)n_units), b->d_units = (BatchUnit *)p;
+    if (!st) st = batch_alloc(b, &p, sizeof(int32_t) * std::max<size_t>(1, h_act.size())), b->d_act = (int32_t *)p;
+    if (!st) st = batch_alloc(b, &p, sizeof(RoundDesc)), b->d_round = (RoundDesc *)p;
+    if (!st) st = batch_alloc(b, &p, sizeof(AnchorRec) * (size_t)std::max<int64_t>(1, b->recs_cap)),
+             b->d_recs = (AnchorRec *)p;
+    if (!st) st = batch_alloc(b, &p, sizeof(unsigned long long)), b->d_counter = (unsigned long long *)p;
+    if (!st) st = batch_alloc(b, &p, sizeof(DevWalk) * std::max<size_t>(1, b->walks.size())),
+             b->d_walks = (DevWalk *)p;
+    for (int u = 0; u < n_units && !st; ++u) {
+        st = batch_alloc(b, &p, sizeof(float2) * (size_t)b->units[u].round_len);
+        b->h_units[u].out = (float2 *)p;
+    }
+    std::vector<DevWalk> h_walks(b->walks.size());
+    for (size_t w = 0; w < b->walks.size() && !st; ++w) {
+        h_walks[w].seed = b->walks[w].seed;
+        h_walks[w].sigma = b->walks[w].sigma;
+        st = batch_alloc(b, &p, sizeof(double) * (size_t)std::max<int64_t>(1, b->walks[w].partial_cap));
+        h_walks[w].partial = (double *)p;
+        if (!st) st = batch_alloc(b, &p, sizeof(double) * (size_t)total_blocks[w]), h_walks[w].totals = (double *)p;
+        if (!st) st = batch_alloc(b, &p, sizeof(double) * (size_t)(total_blocks[w] + 1)), h_walks[w].carry = (double *)p;
+        if (!st && cudaMemsetAsync(h_walks[w].carry, 0, sizeof(double), c->stream) != cudaSuccess)
+            st = fail(c, LPK_ECUDA, "walk carry reset failed");
+    }
+    for (int i = 0; i < 2 && !st; ++i) {
+        if (cudaHostAlloc((void **)&b->h_round[i], sizeof(RoundDesc), cudaHostAllocDefault) != cudaSuccess)
+            st = fail(c, LPK_ENOMEM, "pinned round descriptor allocation failed");
+        else if (cudaEventCreateWithFlags(&b->done[i], cudaEventDisableTiming) != cudaSuccess)
+            st = fail(c, LPK_ECUDA, "event creation failed");
+    }
+    if (!st) {
+        cudaError_t e = cudaMemcpyAsync(b->d_bands, h_bands.data(), sizeof(DevBand) * (size_t)n_units,
+                                        cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(b->d_units, b->h_units.data(), sizeof(BatchUnit) * (size_t)n_units,
+                                cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess && !h_act.empty())
+            e = cudaMemcpyAsync(b->d_act, h_act.data(), sizeof(int32_t) * h_act.size(), cudaMemcpyHostToDevice,
+                                c->stream);
+        if (e == cudaSuccess && !h_walks.empty())
+            e = cudaMemcpyAsync(b->d_walks, h_walks.data(), sizeof(DevWalk) * h_walks.size(), cudaMemcpyHostToDevice,
+                                c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) st = cuda_fail(c, e, "batch upload");
+    }
+    if (!st) {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+        b->walk_grid = sms * 8;
+        b->anchor_grid = sms * 8;
+        st = configure(b, c->split_variant, 0);
+    }
+    if (st) {
+        lpk_batch_destroy(b);
+        return st;
+    }
+    *out = b;
+    return LPK_OK;
+}
+
+int64_t lpk_batch_n_rounds(const lpk_batch *b) { return b ? b->n_rounds : -1; }
+
+lpk_status lpk_batch_round_extent(const lpk_batch *b, int64_t round, int32_t unit, int64_t *i0, int64_t *n) {
+    if (!b) return fail(nullptr, LPK_EINVAL, "batch is NULL");
+    if (unit < 0 || unit >= (int32_t)b->units.size()) return fail(b->ctx, LPK_EINVAL, "unit out of range");
+    if (round < 0) return fail(b->ctx, LPK_EINVAL, "round must be >= 0");
+    int64_t a, m;
+    unit_extent(b, round, unit, a, m);
+    if (i0) *i0 = a;
+    if (n) *n = m;
+    return LPK_OK;
+}
+
+lpk_status lpk_batch_run(lpk_batch *b, int64_t round) {
+    if (!b) return fail(nullptr, LPK_EINVAL, "batch is NULL");
+    lpk_ctx *c = b->ctx;
+    if (round < 0 || round >= b->n_rounds) return fail(c, LPK_EINVAL, "round out of range");
+    cudaSetDevice(c->device);
+    const int p = b->parity;
+    // the descriptor buffer p was last read by the round launched two calls ago
+    cudaError_t e = cudaEventSynchronize(b->done[p]);
+    if (e != cudaSuccess) return cuda_fail(c, e, "batch round wait");
+    int tile = 0;
+    split_variant_info(b->variant, &tile, nullptr, nullptr);
+    plan_round(b, round, tile, *b->h_round[p], true, nullptr, nullptr);
+    lpk_status st = LPK_OK;
+    if (!b->graph[p] && (st = build_graph(b, p))) return st;
+    e = cudaGraphLaunch(b->graph[p], c->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(b->done[p], c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "batch graph launch");
+    c->launches += 2 + (b->walks.empty() ? 0 : 2);
+    b->parity ^= 1;
+    b->last_round = round;
+    return LPK_OK;
+}
+
+lpk_status lpk_batch_output(lpk_batch *b, int32_t unit, const lpk_cf32 **d_out) {
+    if (!b) return fail(nullptr, LPK_EINVAL, "batch is NULL");
+    if (unit < 0 || unit >= (int32_t)b->units.size()) return fail(b->ctx, LPK_EINVAL, "unit out of range");
+    if (!d_out) return fail(b->ctx, LPK_EINVAL, "d_out is NULL");
+    *d_out = (const lpk_cf32 *)b->h_units[unit].out;
+    return LPK_OK;
+}
+
+lpk_status lpk_batch_copy_out(lpk_batch *b, int32_t unit, lpk_cf32 *host, int64_t cap) {
+    if (!b) return fail(nullptr, LPK_EINVAL, "batch is NULL");
+    lpk_ctx *c = b->ctx;
+    if (unit < 0 || unit >= (int32_t)b->units.size()) return fail(c, LPK_EINVAL, "unit out of range");
+    if (b->last_round < 0) return fail(c, LPK_EINVAL, "no round has run");
+    int64_t i0, n;
+    unit_extent(b, b->last_round, unit, i0, n);
+    if (n > 0 && (!host || cap < n)) return fail(c, LPK_EINVAL, "host buffer is NULL or too small");
+    cudaSetDevice(c->device);
+    cudaError_t e = n > 0 ? cudaMemcpyAsync(host, b->h_units[unit].out, sizeof(lpk_cf32) * (size_t)n,
+                                            cudaMemcpyDeviceToHost, c->stream)
+                          : cudaSuccess;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "batch output copy");
+    return LPK_OK;
+}
+
+lpk_status lpk_batch_set_config(lpk_batch *b, int32_t variant, int32_t blocks_per_sm) {
+    if (!b) return fail(nullptr, LPK_EINVAL, "batch is NULL");
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    return configure(b, variant, blocks_per_sm);
+}
+
+lpk_status lpk_batch_get_config(const lpk_batch *b, int32_t *variant, int32_t *bps, int32_t *max_bps) {
+    if (!b) return fail(nullptr, LPK_EINVAL, "batch is NULL");
+    if (variant) *variant = b->variant;
+    if (bps) *bps = b->bps;
+    if (max_bps) *max_bps = b->max_bps;
+    return LPK_OK;
+}
+
+lpk_status lpk_batch_autotune(lpk_batch *b, int64_t round, int32_t reps, double *ms_table) {
+    if (!b) return fail(nullptr, LPK_EINVAL, "batch is NULL");
+    lpk_ctx *c = b->ctx;
+    if (reps < 1) return fail(c, LPK_EINVAL, "reps must be >= 1");
+    if (round < 0 || round >= b->n_rounds) return fail(c, LPK_EINVAL, "round out of range");
+    cudaSetDevice(c->device);
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    double best = 1e300;
+    int best_v = b->variant, best_bps = b->bps;
+    lpk_status st = LPK_OK;
+    for (int v = 0; v < kSplitVariants && !st; ++v) {
+        for (int h = 0; h < 2 && !st; ++h) {
+            if (ms_table) ms_table[2 * v + h] = -1.0;
+            cudaStreamSynchronize(c->stream);
+            if ((st = configure(b, v, 0))) break;
+            const int bps = h == 0 ? b->max_bps : b->max_bps / 2;
+            if (h == 1 && (bps < 1 || bps == b->max_bps)) continue;
+            if ((st = configure(b, v, bps))) break;
+            if ((st = lpk_batch_run(b, round))) break;  // warm-up (and graph build)
+            cudaEventRecord(t0, c->stream);
+            for (int r = 0; r < reps && !st; ++r) st = lpk_batch_run(b, round);
+            cudaEventRecord(t1, c->stream);
+            if (st) break;
+            cudaError_t e = cudaEventSynchronize(t1);
+            if (e != cudaSuccess) { st = cuda_fail(c, e, "autotune timing"); break; }
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, t0, t1);
+            const double per = (double)ms / reps;
+            if (ms_table) ms_table[2 * v + h] = per;
+            if (per < best) {
+                best = per;
+                best_v = v;
+                best_bps = bps;
+            }
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    cudaStreamSynchronize(c->stream);
+    if (st) return st;
+    return configure(b, best_v, best_bps);
+}
+
+}  // extern "C"

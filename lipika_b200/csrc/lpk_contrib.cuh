@@ -5,6 +5,7 @@
 
 #include "../../include/lipika_cuda.h"
 #include "lpk_device.cuh"
+#include "lpk_walk.cuh"
 
 namespace lpk {
 
@@ -13,11 +14,18 @@ __device__ __forceinline__ double band_delta(const DevBand &b, int64_t j, double
         return __dadd_rn(0.0, __dadd_rn(b.clock_offset, __dmul_rn(b.clock_y0, t_local)));
     if (b.clock_mode == LPK_CLOCK_DEVICE_WALK) {  // ClockStream::delta_t_at, clock/mod.rs:329-346
         double x = __dmul_rn(t_local, b.fm);      // elapsed = t - 0.0
-        if (x <= 0.0)
-            return __dadd_rn(__dadd_rn(b.eps[0 - b.eps_k0], 0.0), __dadd_rn(b.clock_offset, __dmul_rn(b.clock_y0, 0.0)));
+        if (x <= 0.0) {
+            double e0 = b.eps[0 - b.eps_k0];
+            if (b.eps_carry) e0 = __dadd_rn(b.eps_carry[0], e0);
+            return __dadd_rn(__dadd_rn(e0, 0.0), __dadd_rn(b.clock_offset, __dmul_rn(b.clock_y0, 0.0)));
+        }
         int64_t k0 = floor_to_i64(x);
         double frac = __dsub_rn(x, (double)k0);
         double lo = b.eps[k0 - b.eps_k0], hi = b.eps[k0 + 1 - b.eps_k0];
+        if (b.eps_carry) {
+            lo = __dadd_rn(b.eps_carry[k0 / kWalkBlock], lo);
+            hi = __dadd_rn(b.eps_carry[(k0 + 1) / kWalkBlock], hi);
+        }
         double eps = __dadd_rn(__dmul_rn(lo, __dsub_rn(1.0, frac)), __dmul_rn(hi, frac));
         return __dadd_rn(__dadd_rn(eps, 0.0), __dadd_rn(b.clock_offset, __dmul_rn(b.clock_y0, t_local)));
     }

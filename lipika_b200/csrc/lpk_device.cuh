@@ -60,6 +60,8 @@ struct DevBand {
     const double *delta;                // n (clock mode HOST)
     const double *rxpos;                // (3, n) (rx PER_SAMPLE)
     const double *eps;                  // walk ε on master indices [eps_k0, ...) (DEVICE_WALK)
+    const double *eps_carry;            // non-NULL: eps holds the in-block prefix P_b(k) and
+                                        // ε(k) = eps_carry[b] ⊕ P_b(k), b the scan block of k
     int64_t eps_k0;
     double fm;                          // master (walk) rate
     float noise_std;                    // sqrt(P/2) as f32; 0 = no noise

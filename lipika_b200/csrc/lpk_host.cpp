@@ -6,6 +6,7 @@
 // Table construction uses glibc libm with no FMA contraction
 // (-ffp-contract=off), as the reference's Rust code does on x86_64 Linux,
 // so trajectory grids and signal tables are bit-identical to its own.
+#include <algorithm>
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
@@ -670,6 +671,94 @@ lpk_status lpk_generate_band(lpk_scene *s, int32_t r, int32_t b, uint64_t seed_b
         }
     }
     res->n_samples = i0;
+    return LPK_OK;
+}
+
+namespace {
+struct UnitSinkAdapter {
+    lpk_unit_sink_fn sink;
+    void *user;
+    int32_t work_idx;
+};
+int32_t unit_sink_adapter(void *user, const lpk_cf32 *chunk, int64_t n) {
+    UnitSinkAdapter *a = (UnitSinkAdapter *)user;
+    return a->sink(a->user, a->work_idx, chunk, n);
+}
+}  // namespace
+
+lpk_status lpk_generate_scene(lpk_scene *s, uint64_t seed_base, double round_s, int32_t flags, lpk_unit_sink_fn sink,
+                              void *user) {
+    if (!s || !sink) return host_fail(LPK_EINVAL, "NULL scene or sink");
+    if (!s->ctx) return host_fail(LPK_EINVAL, "scene was prepared without a context");
+    const int32_t n_work = (int32_t)s->work.size();
+    std::vector<lpk_work_unit> units;
+    std::vector<int32_t> unit_work;  // work index of each batch unit
+    std::vector<std::vector<int32_t>> actives;
+    std::vector<int32_t> rest;  // work units rendered one by one
+    actives.reserve((size_t)n_work);
+    for (int32_t w = 0; w < n_work; ++w) {
+        const int32_t r = s->work[w].first, b = s->work[w].second;
+        lpk_work_unit u;
+        memset(&u, 0, sizeof u);
+        lpk_status st = lpk_scene_band_desc(s, r, b, seed_base, w, &u.band);
+        if (st) return st;
+        if (!(flags & LPK_NOISE_ON)) u.band.noise_power_w = 0.0;
+        if (flags & LPK_GEN_SPLIT) u.band.solver = LPK_SOLVER_SPLIT;
+        const RxHost &rx = s->rx[r];
+        if ((flags & LPK_GEN_DEVICE_CLOCK) && u.band.clock_mode == LPK_CLOCK_HOST && rx.stationary &&
+            !(rx.clock.flicker_floor > 0.0))
+            u.band.clock_mode = LPK_CLOCK_DEVICE_WALK;
+        if (!rx.stationary || u.band.clock_mode == LPK_CLOCK_HOST) {
+            rest.push_back(w);
+            continue;
+        }
+        actives.emplace_back(256);
+        int32_t na = lpk_scene_band_active(s, r, b, actives.back().data(), 256);
+        if (na > 256) return host_fail(LPK_EINVAL, "more than 256 in-band transmitters");
+        u.n_active = na;
+        u.n_samples = lpk_scene_band_samples(s, r, b);
+        units.push_back(u);
+        unit_work.push_back(w);
+    }
+    for (size_t k = 0; k < units.size(); ++k) units[k].active = actives[k].data();
+    if (!units.empty()) {
+        if ((int)units.size() > 256) return host_fail(LPK_EINVAL, "more than 256 batched work units");
+        lpk_batch *batch = nullptr;
+        lpk_status st = lpk_batch_create(s->ctx, units.data(), (int32_t)units.size(), round_s, &batch);
+        if (st) return st;
+        std::unique_ptr<lpk_batch, void (*)(lpk_batch *)> guard(batch, lpk_batch_destroy);
+        const int64_t rounds = lpk_batch_n_rounds(batch);
+        if ((flags & LPK_GEN_AUTOTUNE) && rounds > 0 && (st = lpk_batch_autotune(batch, rounds / 2, 2, nullptr)))
+            return st;
+        int64_t cap = 0;
+        for (size_t k = 0; k < units.size(); ++k) {
+            int64_t i0, n;
+            lpk_batch_round_extent(batch, 0, (int32_t)k, &i0, &n);
+            cap = std::max(cap, n);
+        }
+        std::vector<lpk_cf32> host((size_t)std::max<int64_t>(cap, 1));
+        std::vector<char> stopped(units.size(), 0);
+        for (int64_t rd = 0; rd < rounds; ++rd) {
+            if ((st = lpk_batch_run(batch, rd))) return st;
+            for (size_t k = 0; k < units.size(); ++k) {
+                int64_t i0, n;
+                lpk_batch_round_extent(batch, rd, (int32_t)k, &i0, &n);
+                if (n <= 0 || stopped[k]) continue;
+                if ((st = lpk_batch_copy_out(batch, (int32_t)k, host.data(), (int64_t)host.size()))) return st;
+                int32_t flow = sink(user, unit_work[k], host.data(), n);
+                if (flow < 0) return host_fail(LPK_EINVAL, "sink reported an error");
+                if (flow == 1) stopped[k] = 1;
+            }
+        }
+    }
+    for (int32_t w : rest) {
+        const int32_t r = s->work[w].first, b = s->work[w].second;
+        const int64_t chunk = std::max<int64_t>(1, std::llround(round_s * s->rx[r].bands[b].sample_rate_hz));
+        UnitSinkAdapter a{sink, user, w};
+        lpk_status st = lpk_generate_band(s, r, b, seed_base, w, chunk, flags & ~LPK_GEN_AUTOTUNE, unit_sink_adapter,
+                                          &a, nullptr);
+        if (st) return st;
+    }
     return LPK_OK;
 }
 

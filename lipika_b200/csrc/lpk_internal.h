@@ -8,9 +8,9 @@
 
 #include "../../include/lipika_cuda.h"
 #include "lpk_device.cuh"
+#include "lpk_walk.cuh"
 
 namespace lpk {
-constexpr int64_t kWalkBlock = 4096;  // master samples per clock-walk scan block
 
 // Cached carries of one receiver clock walk (seed, master rate, step σ).
 struct WalkState {
@@ -44,6 +44,7 @@ struct lpk_ctx {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
     size_t prof_used = 0;
     int64_t launches = 0;
+    int split_variant = 0;  // launch shape of the split fan-out (LPK_SPLIT_VARIANTS)
 };
 
 namespace lpk {
@@ -62,13 +63,15 @@ cudaError_t launch_tx_contribution(const DevBand &b, const DevTx *d_tx, int32_t 
                                    double *d_phase, double *d_temit, double *d_range, cudaStream_t s);
 cudaError_t launch_rx_chain(const DevBand &b, float2 *d_iq, cudaStream_t s);
 cudaError_t launch_band_delta(const DevBand &b, double *d_out, cudaStream_t s);
-// Split-precision fan-out (anchor kernel + per-sample kernel); d_recs holds
-// split_recs_bytes(n, n_active) bytes. The dbg arrays (single transmitter
-// only, may be NULL) receive the reduced phase, emission time and delay.
-size_t split_recs_bytes(int64_t i0, int64_t n, int32_t n_active);
-cudaError_t launch_band_split(const DevBand &b, const DevTx *d_tx, const int32_t *d_active, int32_t n_active,
-                              void *d_recs, float2 *d_out, double *dbg_phase, double *dbg_temit, double *dbg_delay,
-                              cudaStream_t s);
+// Split-precision fan-out (anchor kernel + per-sample kernel) in launch
+// shape `variant`; d_recs holds split_recs_bytes(variant, i0, n, n_active)
+// bytes. The dbg arrays (single transmitter only, may be NULL) receive the
+// reduced phase, emission time and delay.
+bool split_variant_info(int variant, int *tile, int *threads, int *min_blocks);
+size_t split_recs_bytes(int variant, int64_t i0, int64_t n, int32_t n_active);
+cudaError_t launch_band_split(int variant, const DevBand &b, const DevTx *d_tx, const int32_t *d_active,
+                              int32_t n_active, void *d_recs, float2 *d_out, double *dbg_phase, double *dbg_temit,
+                              double *dbg_delay, cudaStream_t s);
 // True when the band can take the split path (stationary receiver, no antenna).
 inline bool use_split(const lpk_band_desc *d) {
     return d->solver == LPK_SOLVER_SPLIT && d->rx_kind == LPK_RX_STATIONARY && !d->has_antenna;

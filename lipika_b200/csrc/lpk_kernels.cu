@@ -8,6 +8,7 @@
 // CUDA's sin/cos).
 #include "lpk_internal.h"
 #include "lpk_contrib.cuh"
+#include "lpk_walk.cuh"
 
 namespace lpk {
 
@@ -103,44 +104,21 @@ k_rx_chain(const DevBand b, float2 *__restrict__ iq) {
 }
 
 // ---------------------------------------------------------------- clock walk
-// The walk ε(k) = Σ_{j<=k} σ z_j is defined through fixed scan blocks of
-// kWalkBlock master samples: ε(k) = carry(b) + P_b(k), with P_b the in-block
-// inclusive prefix computed by one fixed parallel order and carry(b) the
-// sequential sum of the totals of blocks 0..b-1. Nothing depends on how the
-// band is chunked, so every chunking reproduces the same ε.
-constexpr int kWalkThreads = 256;
-constexpr int kWalkPer = kWalkBlock / kWalkThreads;  // 16
-
+// One block per scan block (lpk_walk.cuh): its total (totals != NULL), or
+// ε(k) = carry(b) ⊕ P_b(k) for the master indices [kA, kB] it holds.
 __global__ void __launch_bounds__(kWalkThreads)
 k_walk_block(uint64_t seed, double sigma, int64_t b0, double *__restrict__ totals,
              const double *__restrict__ carry, double *__restrict__ eps, int64_t kA, int64_t kB) {
     __shared__ double warp_tot[kWalkThreads / 32];
     const int64_t b = b0 + blockIdx.x;
-    const int64_t base = b * kWalkBlock + (int64_t)threadIdx.x * kWalkPer;
-    double v[kWalkPer];
-    double run = 0.0;
-#pragma unroll
-    for (int i = 0; i < kWalkPer; ++i) {
-        run = __dadd_rn(run, walk_increment(seed, base + i, sigma));
-        v[i] = run;
-    }
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    double incl = run;  // warp inclusive scan of per-thread totals
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        double o = __shfl_up_sync(0xffffffffu, incl, off);
-        if (lane >= off) incl = __dadd_rn(o, incl);
-    }
-    if (lane == 31) warp_tot[wid] = incl;
-    __syncthreads();
-    double wpre = 0.0;
-    for (int w = 0; w < wid; ++w) wpre = __dadd_rn(wpre, warp_tot[w]);
-    const double offset = __dadd_rn(wpre, __dsub_rn(incl, run));  // exclusive prefix of this thread
+    double v[kWalkPer], offset;
+    walk_block_prefix(seed, sigma, b, warp_tot, v, offset);
     if (totals) {
         if (threadIdx.x == kWalkThreads - 1) totals[b] = __dadd_rn(offset, v[kWalkPer - 1]);
         return;
     }
     const double c = carry[b];
+    const int64_t base = b * kWalkBlock + (int64_t)threadIdx.x * kWalkPer;
 #pragma unroll
     for (int i = 0; i < kWalkPer; ++i) {
         int64_t k = base + i;

@@ -12,7 +12,7 @@
 //    The fits are of the unrounded delay; per sample the exact rounding
 //    offset of each query (a TwoSum) times ∂delay/∂t of its segment restores
 //    the staircase.
-// Per (tile of kSplitTile band samples, transmitter) an anchor thread fits
+// Per (tile of band samples, transmitter) an anchor thread fits
 // delay_i(tu) = c0 + Δ(c1 + Δ c2), Δ = tu - tu0, for both iterates from
 // unrounded FP64 solves at three times. Per sample: both query offsets, two
 // polynomials, the signal index in FP64 with a guard band (a sample within
@@ -22,25 +22,35 @@
 // (Cody–Waite), then sin/cos, amplitude and the complex MAC in FP32.
 #pragma once
 
-#include "lpk_device.cuh"
+#include "lpk_contrib.cuh"
 
 namespace lpk {
 
-#ifndef LPK_SPLIT_TILE
-#define LPK_SPLIT_TILE 1024
-#endif
-#ifndef LPK_SPLIT_THREADS
-#define LPK_SPLIT_THREADS 256
-#endif
-constexpr int kSplitTile = LPK_SPLIT_TILE;        // band samples per anchor tile
-constexpr int kSplitThreads = LPK_SPLIT_THREADS;  // kSplitTile / kSplitThreads samples per thread
+// Compiled launch shapes of the fan-out: (index, band samples per tile,
+// threads per block, minimum resident blocks per SM). The minimum-blocks
+// bound caps registers (65536 / (threads x blocks)); tile / threads is the
+// number of samples each thread carries through the transmitter loop.
+#define LPK_SPLIT_VARIANTS(X) \
+    X(0, 1024, 256, 3)        \
+    X(1, 512, 256, 3)         \
+    X(2, 1024, 512, 2)        \
+    X(3, 512, 256, 4)         \
+    X(4, 1024, 256, 2)        \
+    X(5, 1024, 512, 1)
+constexpr int kSplitVariants = 6;
+constexpr int kSplitMaxTile = 1024;
+constexpr int kSplitMinTile = 512;
 // Tiles are aligned to absolute band-sample indices and fitted over a tu range
 // that depends only on the tile and the clock's deterministic trend, widened
 // by kSplitMargin; a sample whose tu falls outside takes the exact path. So
 // the fit, and every output bit, is independent of how the band is chunked.
 constexpr double kSplitMargin = 1e-5;  // s
 
-enum : int32_t { kRecExact = 1, kRecNavConst = 2, kRecGateOff = 4 };
+// kRecExact: the whole tile takes the exact path; kRecNavVary: a C/A nav bit
+// boundary falls inside the tile (otherwise nav_pm holds the tile's sign);
+// kRecGateOff: the transmitter is silent over the whole tile (gate off, or
+// an empty frame), so it adds nothing.
+enum : int32_t { kRecExact = 1, kRecNavVary = 2, kRecGateOff = 4 };
 
 struct __align__(16) AnchorRec {
     double tu0, tu_hi;                // fit range; Δ origin tu0
@@ -54,7 +64,7 @@ struct __align__(16) AnchorRec {
     double guard;                     // emission-time guard band (s)
     float amp0, amp1;                 // amplitude = amp0 + amp1 Δ
     int32_t flags;
-    int32_t nav_pm;                   // constant nav sign of the tile (kRecNavConst)
+    int32_t nav_pm;                   // nav sign of the tile (1 with nav off; unused with kRecNavVary)
     int64_t sym_raw0, sym_pos0;       // framed kinds: raw symbol count at the tile start and its frame slot
 };
 
@@ -138,6 +148,388 @@ __device__ __forceinline__ int64_t frame_slot(const DevTx &tx, int64_t raw, int6
     int64_t p = pos0 + (raw - raw0);
     if (p >= tx.n_sym || p < 0) p = i64_rem_euclid(p, tx.n_sym);
     return p;
+}
+
+constexpr double kSplitInf = __builtin_huge_val();
+
+// Fit one (tile, transmitter): band samples gs..ge (absolute indices) of
+// band b. Everything depends only on the tile's absolute position, the
+// transmitter and the clock's deterministic trend, never on chunking.
+// exact_only: the tile takes the reference-exact path for every sample
+// (fan-out under the plain FP64 solver, or with an antenna).
+__device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, int64_t gs, int64_t ge, bool exact_only,
+                                           AnchorRec &r) {
+    const double tls = (double)gs / b.fs, tle = (double)ge / b.fs;
+    const double tus = tls - (b.clock_offset + b.clock_y0 * tls) - kSplitMargin;
+    const double tue = tle - (b.clock_offset + b.clock_y0 * tle) + kSplitMargin;
+    const double ox = b.rx[0], oy = b.rx[1], oz = b.rx[2];
+    const double h = 0.5 * (tue - tus);
+    const double de = tx.traj_kind != 0 ? b.epoch - tx.t0 : 0.0;
+    r.tu0 = tus;
+    r.tu_hi = tue;
+    r.node0 = r.node1 = kSplitInf;
+    r.tau_if = kTau * (tx.carrier - b.lo);
+    r.flags = 0;
+    r.nav_pm = 1;
+    r.k0 = r.k1a = r.k1b = 0.0;
+    for (int i = 0; i < 3; ++i) r.p0a[i] = r.p0b[i] = r.p1a[i] = r.p1b[i] = 0.0;
+    int64_t lo0s = 0, lo0e = 0, lo1s = 0, lo1e = 0;
+    bool exact = exact_only;
+    if (exact) {
+        r.amp0 = r.amp1 = 0.0f;
+        r.guard = r.ulp_q = r.tie = 0.0;
+        r.sym_raw0 = r.sym_pos0 = 0;
+        r.flags = kRecExact;
+        return;
+    }
+    if (tx.traj_kind != 0) {
+        bool c1, c2, c3, c4;
+        lo0s = seg_unrounded(tx, tus - kEmissionLag, de, c1);
+        lo0e = seg_unrounded(tx, tue - kEmissionLag, de, c2);
+        double d0s = iterate_unrounded(tx, tus, tus - kEmissionLag, de, lo0s, ox, oy, oz, b.inv_c, nullptr, nullptr);
+        double d0e = iterate_unrounded(tx, tue, tue - kEmissionLag, de, lo0e, ox, oy, oz, b.inv_c, nullptr, nullptr);
+        lo1s = seg_unrounded(tx, tus - d0s, de, c3);
+        lo1e = seg_unrounded(tx, tue - d0e, de, c4);
+        exact = c1 || c2 || c3 || c4 || lo0e < lo0s || lo0e > lo0s + 1 || lo1e < lo1s || lo1e > lo1s + 1;
+        if (lo0e != lo0s) r.node0 = tx.t0 + (double)lo0e * tx.dt;
+        if (lo1e != lo1s) r.node1 = tx.t0 + (double)lo1e * tx.dt;
+    }
+    double rs = 1.0, re = 1.0, te_s = tus, te_e = tue;
+    if (!exact) {
+        double v[3];
+        for (int piece = 0; piece < 2; ++piece) {
+            int64_t lo = piece ? lo0e : lo0s;
+            if (piece && lo0e == lo0s) break;
+            for (int i = 0; i < 3; ++i) {
+                double tu = tus + i * h;
+                v[i] = iterate_unrounded(tx, tu, tu - kEmissionLag, de, lo, ox, oy, oz, b.inv_c, nullptr, nullptr);
+            }
+            quad3(v[0], v[1], v[2], h, piece ? r.p0b : r.p0a);
+        }
+        for (int piece = 0; piece < 2; ++piece) {
+            int64_t lo = piece ? lo1e : lo1s;
+            if (piece && lo1e == lo1s) break;
+            for (int i = 0; i < 3; ++i)
+                v[i] = solve_unrounded(tx, tus + i * h, de, lo, ox, oy, oz, b.inv_c, nullptr, nullptr);
+            quad3(v[0], v[1], v[2], h, piece ? r.p1b : r.p1a);
+        }
+        // ∂delay/∂(query time) of each piece at the tile middle
+        bool cl;
+        const double mid = tus + h;
+        const double tq0 = mid - kEmissionLag;
+        double d0m = iterate_unrounded(tx, mid, tq0, de, seg_unrounded(tx, tq0, de, cl), ox, oy, oz, b.inv_c,
+                                       nullptr, &r.k0);
+        iterate_unrounded(tx, mid, mid - d0m, de, lo1s, ox, oy, oz, b.inv_c, nullptr, &r.k1a);
+        r.k1b = r.k1a;
+        if (lo1e != lo1s) iterate_unrounded(tx, mid, mid - d0m, de, lo1e, ox, oy, oz, b.inv_c, nullptr, &r.k1b);
+        solve_unrounded(tx, tus, de, lo1s, ox, oy, oz, b.inv_c, nullptr, &rs);
+        solve_unrounded(tx, tue, de, lo1e, ox, oy, oz, b.inv_c, nullptr, &re);
+        te_s = tus - poly2(r.p1a, 0.0);
+        te_e = tue - poly2(lo1e != lo1s ? r.p1b : r.p1a, 2.0 * h);
+    }
+    const float amp_s = (float)(tx.amp_factor / rs), amp_e = (float)(tx.amp_factor / re);
+    r.amp0 = amp_s;
+    r.amp1 = (tue > tus) ? (amp_e - amp_s) / (float)(tue - tus) : 0.0f;
+    r.guard = ldexp(16.0, ilogb(fmax(fmax(fabs(te_s), fabs(te_e)), 1.0)) - 52);
+    // The second query epoch + t1 rounds to ulp_q; our t1 may differ from the
+    // reference's by a few ulp of t1, so a sum within `tie` of a rounding
+    // midpoint takes the exact path. When ulp_q is that fine the rounding is
+    // immaterial (< 1e-19 s of delay) and the check is off (tie < 0).
+    r.ulp_q = ldexp(1.0, ilogb(fmax(fmax(fabs(b.epoch + tus), fabs(b.epoch + tue)), 1e-300)) - 52);
+    const double tie = ldexp(8.0, ilogb(fmax(fmax(fabs(tus), fabs(tue)), 1.0)) - 52);
+    r.tie = (8.0 * tie > r.ulp_q) ? -1.0 : tie;
+    r.sym_raw0 = 0;
+    r.sym_pos0 = 0;
+    if (!exact && (tx.sig_kind == kBpsk || tx.sig_kind == kOok || tx.sig_kind == kQam16)) {
+        if (tx.n_sym <= 0) {
+            r.flags |= kRecGateOff;  // an empty frame is silent everywhere
+        } else {
+            r.sym_raw0 = floor_to_i64((te_s - tx.epoch_rel) * tx.rate);
+            r.sym_pos0 = tx.has_repeat
+                             ? i64_rem_euclid((int64_t)((uint64_t)r.sym_raw0 + (uint64_t)tx.repeat_from), tx.n_sym)
+                             : r.sym_raw0;
+            // the per-sample slot wraps at most once: the tile must span
+            // fewer symbols than the frame holds
+            if (tx.has_repeat && !((te_e - te_s) * tx.rate + 3.0 < (double)tx.n_sym)) exact = true;
+        }
+    }
+    if (!exact && tx.sig_kind == kCa && tx.nav_kind != kNavOff) {
+        double ns = (te_s - tx.epoch_rel) * kNavBitRate, ne = (te_e - tx.epoch_rel) * kNavBitRate;
+        double fs_ = floor(ns), fe_ = floor(ne), g = r.guard * kNavBitRate;
+        if (fs_ == fe_ && ns - fs_ > g && ne - fe_ < 1.0 - g) {
+            int64_t bi = (int64_t)fs_;
+            int nav = 1;
+            if (tx.nav_kind == kNavDummy) nav = nav_bit_pm(tx.nav_seed, bi);
+            else if (tx.nav_n > 0) nav = tx.nav_bits[bi < 0 ? 0 : (bi < tx.nav_n ? bi : tx.nav_n - 1)];
+            r.nav_pm = nav;
+        } else {
+            r.flags |= kRecNavVary;
+        }
+    }
+    if (!exact && tx.has_gate) {  // a burst edge inside the tile's emission span -> exact tile
+        double span = te_e - te_s, g = r.guard;
+        double u = f64_rem_euclid(te_s + tx.gate_phase, tx.gate_period);
+        for (int i = 0; i < tx.gate_n && !exact; ++i) {
+            double2 on = tx.gate_on[i];
+            for (int e = 0; e < 2 && !exact; ++e) {
+                double edge = e ? on.y : on.x;
+                for (int w = -1; w <= 1; ++w) {
+                    double x = edge + w * tx.gate_period;
+                    if (x >= u - g && x <= u + span + g) { exact = true; break; }
+                }
+            }
+        }
+        if (!exact && !gate_is_on(tx, te_s)) r.flags |= kRecGateOff;
+    }
+    if (exact) r.flags = kRecExact;
+}
+
+// Per-sample values shared by every transmitter of the band: local
+// reception time, clock offset, and the rounding offset of the first
+// trajectory query epoch + (tu - 70 ms), the same for every transmitter.
+struct SampleCtx {
+    double tl, dl, q0;
+};
+
+// Per-(tile, transmitter) code paths of the fast pass, chosen outside the
+// per-sample loop so that the loop body has no branches.
+enum PassKind : int { kPassCa = 0, kPassCaNav, kPassBpsk, kPassOok, kPassQam, kPassCw };
+
+__device__ __forceinline__ int pass_kind(const DevTx &tx, const AnchorRec &r) {
+    switch (tx.sig_kind) {
+    case kCa: return (r.flags & kRecNavVary) ? kPassCaNav : kPassCa;
+    case kBpsk: return kPassBpsk;
+    case kOok: return kPassOok;
+    case kQam16: return kPassQam;
+    default: return kPassCw;
+    }
+}
+
+// Baseband at emission time te; clears ok within the guard band of a chip /
+// bit / symbol boundary (those samples take the exact path).
+template <int K>
+__device__ __forceinline__ void split_baseband(const DevTx &tx, const AnchorRec &R, double te, double guard, bool &ok,
+                                               float &bre, float &bim) {
+    bim = 0.0f;
+    if constexpr (K == kPassCa || K == kPassCaNav) {  // ca_code.rs:167-193
+        const double dt = __dsub_rn(te, tx.epoch_rel);
+        const double cp = __dmul_rn(dt, kCaChipRate);
+        const double fl = floor(cp), fr = cp - fl, g = guard * kCaChipRate;
+        ok &= fr >= g && fr <= 1.0 - g && fabs(fl) <= 1.0e9;
+        int nav = R.nav_pm;
+        if constexpr (K == kPassCaNav) {
+            const double nb = __dmul_rn(dt, kNavBitRate), nfl = floor(nb), nfr = nb - nfl, g2 = guard * kNavBitRate;
+            ok &= nfr >= g2 && nfr <= 1.0 - g2;
+            const int64_t bi = (int64_t)nfl;
+            if (tx.nav_kind == kNavDummy) nav = nav_bit_pm(tx.nav_seed, bi);
+            else nav = tx.nav_n == 0 ? 1 : tx.nav_bits[bi < 0 ? 0 : (bi < tx.nav_n ? bi : tx.nav_n - 1)];
+        }
+        int m = (int)fmax(fmin(fl, 1.0e9), -1.0e9) % 1023;
+        m += m < 0 ? 1023 : 0;
+        const int chip = ((tx.chip_neg[m >> 5] >> (m & 31)) & 1u) ? -nav : nav;
+        bre = (float)chip;
+    } else if constexpr (K == kPassBpsk || K == kPassOok || K == kPassQam) {  // frame_index, signal/mod.rs:109-115
+        const double f = __dmul_rn(__dsub_rn(te, tx.epoch_rel), tx.rate);
+        const double fl = floor(f), fr = f - fl, g = guard * tx.rate;
+        ok &= fr >= g && fr <= 1.0 - g && fabs(fl) <= 9.0e15;
+        const int64_t raw = (int64_t)fl, n = tx.n_sym;
+        int64_t p = R.sym_pos0 + (raw - R.sym_raw0);  // repeating frame: at most one wrap per tile
+        p -= p >= n ? n : 0;
+        p += p < 0 ? n : 0;
+        const bool on = tx.has_repeat ? true : (raw >= 0 && raw < n);
+        p = tx.has_repeat ? p : raw;
+        p = p < 0 ? 0 : (p >= n ? n - 1 : p);  // keeps the load in bounds; `on` masks the value
+        if constexpr (K == kPassBpsk) {
+            bre = on ? (float)__ldg(tx.pm + p) : 0.0f;
+        } else if constexpr (K == kPassOok) {
+            bre = on ? (float)__ldg(tx.ook + p) : 0.0f;
+        } else {
+            const float2 v = __ldg(tx.sym + p);
+            bre = on ? v.x : 0.0f;
+            bim = on ? v.y : 0.0f;
+        }
+    } else {  // CW: the reference rounds ω·t to f32 before an f32 sin/cos (cw.rs:45-50)
+        const float ph = tx.cw_anchored
+                             ? (float)f64_rem_euclid(__dadd_rn(__dmul_rn(tx.cw_omega, te), tx.cw_phase0), kTau)
+                             : (float)__dmul_rn(tx.cw_omega, te);
+        sincosf(ph, &bim, &bre);
+    }
+}
+
+// One transmitter over the thread's S samples (the fast path), without
+// branches in the sample loop. A sample within `tie` of a rounding tie of
+// the second query, or within the guard band of an index boundary, sets
+// its bit in `redo` and is left to the exact path; `fit` has the bits of
+// the samples inside the tile's fit range. DBG stores the diagnostics.
+template <int K, bool DBG, bool KINK, int S, int THREADS>
+__device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, double epoch, const SampleCtx *sc,
+                                           unsigned fit, float *ar, float *ai, unsigned &redo, int64_t first,
+                                           double *dbg_phase, double *dbg_temit, double *dbg_delay) {
+    const double tu0 = R.tu0, node0 = R.node0, node1 = R.node1, k0 = R.k0, tie = R.tie;
+    const double half = 0.5 * R.ulp_q, tau_if = R.tau_if, nts = tx.neg_tau_src, guard = R.guard;
+    const float amp0 = R.amp0, amp1 = R.amp1;
+    // one piece per iterate (no grid node inside the tile): coefficients in registers
+    const double a0 = R.p0a[0], a1 = R.p0a[1], a2 = R.p0a[2], b0 = R.p1a[0], b1 = R.p1a[1], b2 = R.p1a[2];
+    const double ka = R.k1a;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const SampleCtx &c = sc[s];
+        const double tu = __dsub_rn(c.tl, c.dl);  // src/pipeline.rs:927
+        const double d = tu - tu0;
+        double t1s, poly1, k1;
+        if constexpr (KINK) {
+            const double *p0 = __dadd_rn(epoch, __dsub_rn(tu, kEmissionLag)) >= node0 ? R.p0b : R.p0a;
+            t1s = tu - fma(d, fma(d, p0[2], p0[1]), p0[0]);
+        } else {
+            t1s = tu - fma(d, fma(d, a2, a1), a0);
+        }
+        const double t1r = fma(-k0, c.q0, t1s);  // the reference's t1
+        const double s1 = __dadd_rn(epoch, t1r);  // its second query
+        const double e1 = __dsub_rn(s1, epoch);
+        bool ok = fabs(fabs(e1 - t1r) - half) > tie;
+        if constexpr (KINK) {
+            const bool pb = s1 >= node1;
+            const double *p1 = pb ? R.p1b : R.p1a;
+            poly1 = fma(d, fma(d, p1[2], p1[1]), p1[0]);
+            k1 = pb ? R.k1b : R.k1a;
+        } else {
+            poly1 = fma(d, fma(d, b2, b1), b0);
+            k1 = ka;
+        }
+        const double delay = fma(k1, e1 - t1s, poly1);
+        const double te = tu - delay;
+        float bre, bim;
+        split_baseband<K>(tx, R, te, guard, ok, bre, bim);
+        // carrier phase −2π f (delay + Δt) + 2π (f − f_lo) t_local, reduced mod 2π
+        // (Cody–Waite: 2π to 24 bits, kq·hi exact, then 2π − hi); the f32
+        // rounding of the reduced phase is < 1.2e-7 rad, below __sincosf's own error
+        const double phase = fma(tau_if, c.tl, nts * (delay + c.dl));
+        const double kq = rint(phase * 0.15915494309189535);
+        double rr = fma(-kq, 6.2831854820251465, phase);
+        rr = fma(-kq, -1.748455600074497e-07, rr);
+        float sn, cs;
+        __sincosf((float)rr, &sn, &cs);
+        // f32 arithmetic spelled out (no contraction choices left to the
+        // compiler), so every kernel that inlines this pass agrees bit for bit
+        const float amp = __fmaf_rn(amp1, __double2float_rn(d), amp0);
+        const float vre = __fmaf_rn(bre, cs, __fmul_rn(-bim, sn)), vim = __fmaf_rn(bre, sn, __fmul_rn(bim, cs));
+        ok &= (fit >> s) & 1u;
+        ar[s] = ok ? __fmaf_rn(amp, vre, ar[s]) : ar[s];
+        ai[s] = ok ? __fmaf_rn(amp, vim, ai[s]) : ai[s];
+        redo |= (unsigned)!ok << s;
+        if constexpr (DBG) {
+            if ((fit >> s) & 1u) {
+                const int64_t j = first + s * THREADS + threadIdx.x;
+                dbg_phase[j] = rr;
+                dbg_temit[j] = te;
+                dbg_delay[j] = delay;
+            }
+        }
+    }
+}
+
+// One tile of S * THREADS band samples starting at chunk index `first`,
+// with the tile's transmitters and anchor records staged in shared memory.
+// Samples outside [0, b.n) are skipped; the transmitters are summed in
+// active-list order and the epilogue (AWGN, receiver chain) is applied.
+template <int S, int THREADS, bool DBG>
+__device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, const AnchorRec *srec, int n_active,
+                                           int64_t first, float2 *__restrict__ out, double *dbg_phase,
+                                           double *dbg_temit, double *dbg_delay) {
+    SampleCtx sc[S];
+    float ar[S], ai[S];
+    unsigned live = 0, fit = 0;
+    const double tu0 = n_active > 0 ? srec[0].tu0 : 0.0, tu_hi = n_active > 0 ? srec[0].tu_hi : 0.0;
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int64_t j = first + s * THREADS + threadIdx.x;
+        const bool lv = j >= 0 && j < b.n;
+        ar[s] = ai[s] = 0.0f;
+        sc[s] = SampleCtx{0.0, 0.0, 0.0};
+        if (lv) {
+            const double tl = __ddiv_rn((double)(b.i0 + j), b.fs);  // src/pipeline.rs:918
+            const double dl = band_delta(b, j, tl);
+            const double tu = __dsub_rn(tl, dl);                     // :927
+            const double t0q = __dsub_rn(tu, kEmissionLag);
+            const double s0 = __dadd_rn(b.epoch, t0q);
+            sc[s] = SampleCtx{tl, dl, __dsub_rn(__dsub_rn(s0, b.epoch), t0q)};
+            live |= 1u << s;
+            // the fit range depends only on the tile: the same for every transmitter
+            fit |= (unsigned)(tu >= tu0 && tu <= tu_hi) << s;
+        }
+    }
+    for (int k = 0; k < n_active; ++k) {
+        const AnchorRec &R = srec[k];
+        const bool gate_off = (R.flags & kRecGateOff) != 0;
+        if (gate_off && !DBG) continue;
+        const DevTx &T = stx[k];
+        unsigned redo = live;
+        if (!(R.flags & kRecExact) && !gate_off) {
+            redo = 0;
+            const bool kink = R.node0 < kSplitInf || R.node1 < kSplitInf;  // uniform over the block
+#define LPK_PASS(KIND)                                                                                           \
+    do {                                                                                                         \
+        if (kink)                                                                                                \
+            split_pass<KIND, DBG, true, S, THREADS>(T, R, b.epoch, sc, fit, ar, ai, redo, first, dbg_phase,      \
+                                                    dbg_temit, dbg_delay);                                       \
+        else                                                                                                     \
+            split_pass<KIND, DBG, false, S, THREADS>(T, R, b.epoch, sc, fit, ar, ai, redo, first, dbg_phase,     \
+                                                     dbg_temit, dbg_delay);                                      \
+    } while (0)
+            switch (pass_kind(T, R)) {
+            case kPassCa: LPK_PASS(kPassCa); break;
+            case kPassCaNav: LPK_PASS(kPassCaNav); break;
+            case kPassBpsk: LPK_PASS(kPassBpsk); break;
+            case kPassOok: LPK_PASS(kPassOok); break;
+            case kPassQam: LPK_PASS(kPassQam); break;
+            default: LPK_PASS(kPassCw); break;
+            }
+#undef LPK_PASS
+            redo &= live;
+        }
+        if (redo == 0) continue;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {  // the exact path: rare samples, or whole exact tiles
+            if (!((redo >> s) & 1u)) continue;
+            float cr = 0.0f, ci = 0.0f;
+            double ph = 0.0, te = 0.0, rg = 0.0;
+            contribution(T, b, sc[s].tl, __dsub_rn(sc[s].tl, sc[s].dl), sc[s].dl, b.rx[0], b.rx[1], b.rx[2], cr, ci,
+                         &ph, &te, &rg);
+            if (!gate_off) {
+                ar[s] = __fadd_rn(ar[s], cr);
+                ai[s] = __fadd_rn(ai[s], ci);
+            }
+            if constexpr (DBG) {
+                const int64_t j = first + s * THREADS + threadIdx.x;
+                dbg_phase[j] = ph;
+                dbg_temit[j] = te;
+                dbg_delay[j] = rg * b.inv_c;
+            }
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+        const int64_t j = first + s * THREADS + threadIdx.x;
+        if ((live >> s) & 1u) out[j] = band_epilogue(b, ar[s], ai[s], b.i0 + j);
+    }
+}
+
+// Stage the tile's transmitters and anchor records into shared memory
+// (8-byte words, all threads of the block).
+__device__ __forceinline__ void stage_tile(const DevTx *__restrict__ txs, const int32_t *__restrict__ active,
+                                           int n_active, const AnchorRec *__restrict__ recs, DevTx *stx,
+                                           AnchorRec *srec, bool load_tx) {
+    const int wt = (int)(sizeof(DevTx) / 8), wr = (int)(sizeof(AnchorRec) / 8);
+    if (load_tx) {
+        for (int k = 0; k < n_active; ++k) {
+            const uint64_t *src = reinterpret_cast<const uint64_t *>(txs + active[k]);
+            uint64_t *dst = reinterpret_cast<uint64_t *>(stx + k);
+            for (int w = threadIdx.x; w < wt; w += blockDim.x) dst[w] = src[w];
+        }
+    }
+    const uint64_t *rsrc = reinterpret_cast<const uint64_t *>(recs);
+    uint64_t *rdst = reinterpret_cast<uint64_t *>(srec);
+    for (int w = threadIdx.x; w < wr * n_active; w += blockDim.x) rdst[w] = rsrc[w];
 }
 
 }  // namespace lpk

@@ -28,7 +28,7 @@ LPK_CLOCK_HOST, LPK_CLOCK_DETERMINISTIC, LPK_CLOCK_DEVICE_WALK = 0, 1, 2
 LPK_RX_STATIONARY, LPK_RX_PER_SAMPLE = 0, 1
 LPK_POST_GAIN, LPK_POST_NONLINEARITY, LPK_POST_ADC = 0, 1, 2
 LPK_SOLVER_REFERENCE, LPK_SOLVER_SPLIT = 0, 1
-LPK_NOISE_OFF, LPK_NOISE_ON, LPK_GEN_DEVICE_CLOCK, LPK_GEN_SPLIT = 0, 1, 2, 4
+LPK_NOISE_OFF, LPK_NOISE_ON, LPK_GEN_DEVICE_CLOCK, LPK_GEN_SPLIT, LPK_GEN_AUTOTUNE = 0, 1, 2, 4, 8
 
 
 class LpkError(RuntimeError):
@@ -88,7 +88,13 @@ class BandResult(C.Structure):
                 ("unoccluded", C.c_uint8 * 256)]
 
 
+class WorkUnit(C.Structure):
+    _fields_ = [("band", BandDesc), ("active", C.POINTER(C.c_int32)), ("n_active", C.c_int32),
+                ("reserved", C.c_int32), ("n_samples", C.c_int64)]
+
+
 SINK_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.POINTER(CF32), C.c_int64)
+UNIT_SINK_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.c_int32, C.POINTER(CF32), C.c_int64)
 
 _D = C.POINTER(C.c_double)
 _I32 = C.POINTER(C.c_int32)
@@ -120,6 +126,20 @@ SIGNATURES = {
                                         _D, _D, _D]),
     "lpk_clock_device_delta": (C.c_int32, [_VP, C.POINTER(BandDesc), C.c_int64, C.c_int64, _D]),
     "lpk_rx_chain_apply": (C.c_int32, [_VP, C.POINTER(BandDesc), _CF, C.c_int64]),
+    "lpk_split_variant_count": (C.c_int32, []),
+    "lpk_split_variant_info": (C.c_int32, [C.c_int32, _I32, _I32, _I32]),
+    "lpk_ctx_set_split_variant": (C.c_int32, [_VP, C.c_int32]),
+    "lpk_ctx_split_variant": (C.c_int32, [_VP]),
+    "lpk_batch_create": (C.c_int32, [_VP, C.POINTER(WorkUnit), C.c_int32, C.c_double, C.POINTER(_VP)]),
+    "lpk_batch_destroy": (None, [_VP]),
+    "lpk_batch_n_rounds": (C.c_int64, [_VP]),
+    "lpk_batch_round_extent": (C.c_int32, [_VP, C.c_int64, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "lpk_batch_run": (C.c_int32, [_VP, C.c_int64]),
+    "lpk_batch_output": (C.c_int32, [_VP, C.c_int32, C.POINTER(_VP)]),
+    "lpk_batch_copy_out": (C.c_int32, [_VP, C.c_int32, _CF, C.c_int64]),
+    "lpk_batch_set_config": (C.c_int32, [_VP, C.c_int32, C.c_int32]),
+    "lpk_batch_get_config": (C.c_int32, [_VP, _I32, _I32, _I32]),
+    "lpk_batch_autotune": (C.c_int32, [_VP, C.c_int64, C.c_int32, _D]),
     "lpk_scene_prepare": (C.c_int32, [_VP, C.POINTER(A.SceneCfg), C.POINTER(_VP)]),
     "lpk_scene_free": (None, [_VP]),
     "lpk_scene_n_work": (C.c_int32, [_VP]),
@@ -132,6 +152,7 @@ SIGNATURES = {
                                       SINK_FN, _VP, C.POINTER(BandResult)]),
     "lpk_generate_band_to_file": (C.c_int32, [_VP, C.c_int32, C.c_int32, C.c_uint64, C.c_int32, C.c_int64,
                                               C.c_int32, C.c_char_p, C.POINTER(BandResult)]),
+    "lpk_generate_scene": (C.c_int32, [_VP, C.c_uint64, C.c_double, C.c_int32, UNIT_SINK_FN, _VP]),
     "lpk_clock_new": (C.c_int32, [C.POINTER(A.ClockCfg), C.c_double, C.c_double, C.c_uint64, C.POINTER(_VP)]),
     "lpk_clock_delta_t": (C.c_int32, [_VP, _D, C.c_int64, _D]),
     "lpk_clock_free": (None, [_VP]),
@@ -198,3 +219,89 @@ class Context:
 
     def check(self, code):
         check(code, self.h)
+
+
+def split_variants():
+    """[(tile, threads, min_blocks)] of every compiled split launch shape."""
+    L = lib()
+    out = []
+    for v in range(L.lpk_split_variant_count()):
+        t, n, m = C.c_int32(), C.c_int32(), C.c_int32()
+        check(L.lpk_split_variant_info(v, C.byref(t), C.byref(n), C.byref(m)))
+        out.append((t.value, n.value, m.value))
+    return out
+
+
+class Batch:
+    """An lpk_batch: work units (band descriptor, active list, length) of a
+    scene rendered together, one graph-replayed round at a time."""
+
+    def __init__(self, ctx: Context, units, round_s: float):
+        """units: iterable of (BandDesc, active int sequence, n_samples)."""
+        self.ctx = ctx
+        self._act = []
+        arr = (WorkUnit * len(units))()
+        for k, (band, active, n) in enumerate(units):
+            a = np.ascontiguousarray(np.asarray(active, dtype=np.int32))
+            self._act.append(a)
+            arr[k].band = band
+            arr[k].active = a.ctypes.data_as(_I32) if a.size else None
+            arr[k].n_active = int(a.size)
+            arr[k].n_samples = int(n)
+        h = _VP()
+        ctx.check(lib().lpk_batch_create(ctx.h, arr, len(units), float(round_s), C.byref(h)))
+        self.h = h
+        self.n_units = len(units)
+        self.n_rounds = int(lib().lpk_batch_n_rounds(h))
+        self._caps = [max([self.extent(r, u)[1] for r in range(min(self.n_rounds, 2))] + [1])
+                      for u in range(self.n_units)]
+
+    def close(self):
+        if getattr(self, "h", None):
+            try:
+                lib().lpk_batch_destroy(self.h)
+            except Exception:
+                pass
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def extent(self, rnd: int, unit: int):
+        i0, n = C.c_int64(), C.c_int64()
+        self.ctx.check(lib().lpk_batch_round_extent(self.h, rnd, unit, C.byref(i0), C.byref(n)))
+        return i0.value, n.value
+
+    def run(self, rnd: int):
+        self.ctx.check(lib().lpk_batch_run(self.h, rnd))
+
+    def output(self, unit: int) -> np.ndarray:
+        """Copy of unit's output of the last round (complex64)."""
+        buf = np.zeros(self._caps[unit], dtype=np.complex64)
+        self.ctx.check(lib().lpk_batch_copy_out(self.h, unit, buf.ctypes.data_as(_CF), buf.size))
+        return buf
+
+    def config(self):
+        v, b, m = C.c_int32(), C.c_int32(), C.c_int32()
+        self.ctx.check(lib().lpk_batch_get_config(self.h, C.byref(v), C.byref(b), C.byref(m)))
+        return v.value, b.value, m.value
+
+    def set_config(self, variant: int, blocks_per_sm: int = 0):
+        self.ctx.check(lib().lpk_batch_set_config(self.h, variant, blocks_per_sm))
+
+    def autotune(self, rnd: int = 0, reps: int = 2):
+        nv = lib().lpk_split_variant_count()
+        tab = np.zeros(2 * nv, dtype=np.float64)
+        self.ctx.check(lib().lpk_batch_autotune(self.h, rnd, reps, tab.ctypes.data_as(_D)))
+        return tab.reshape(nv, 2)
+
+    def render(self):
+        """Every round; returns one complex64 array per unit."""
+        outs = [[] for _ in range(self.n_units)]
+        for r in range(self.n_rounds):
+            self.run(r)
+            for u in range(self.n_units):
+                n = self.extent(r, u)[1]
+                if n > 0:
+                    outs[u].append(self.output(u)[:n].copy())
+        return [np.concatenate(o) if o else np.zeros(0, np.complex64) for o in outs]

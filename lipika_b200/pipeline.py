@@ -169,6 +169,30 @@ class Prepared:
         N.check(code, self.ctx.h)
         return res
 
+    def generate_scene(self, seed: int, round_s: float, sink: Callable[[int, np.ndarray], bool],
+                       noise: bool = True, device_clock: bool = True, split: bool = True,
+                       autotune: bool = False) -> None:
+        """Every work unit at once through the batched fan-out
+        (lpk_generate_scene): `sink(work_idx, chunk)` receives each unit's
+        chunks in order and returns True to stop that unit."""
+        err: list = []
+
+        def _sink(_user, w, ptr, n):
+            try:
+                arr = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_float)), shape=(2 * n,)).copy()
+                return 1 if sink(int(w), arr.view(np.complex64)) else 0
+            except BaseException as e:
+                err.append(e)
+                return -1
+
+        cb = N.UNIT_SINK_FN(_sink)
+        flags = (N.LPK_NOISE_ON if noise else N.LPK_NOISE_OFF) | (N.LPK_GEN_DEVICE_CLOCK if device_clock else 0) \
+            | (N.LPK_GEN_SPLIT if split else 0) | (N.LPK_GEN_AUTOTUNE if autotune else 0)
+        code = N.lib().lpk_generate_scene(self.h, seed & 0xFFFFFFFFFFFFFFFF, float(round_s), flags, cb, None)
+        if err:
+            raise err[0]
+        N.check(code, self.ctx.h)
+
     def band_meta(self, r: int, b: int, contributing_idx) -> dict:
         rx = self.scene.receivers[r]
         band = rx.bands[b]

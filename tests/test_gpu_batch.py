@@ -1,0 +1,163 @@
+"""The batched fan-out (lpk_batch_*, lpk_generate_scene) against the
+single-band entry points on the same scenes and seeds.
+
+The batch renders every (receiver, band) work unit in rounds of equal time;
+its outputs must not depend on that: with the reference solver they equal
+lpk_band_chunk bit for bit (same exact arithmetic, same walk values from
+the shared per-receiver walk), with the split solver they equal the
+single-band split kernel of the same launch shape, and any round length or
+round order gives the same bits.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from lipika_b200 import native as N
+from lipika_b200 import pipeline as P
+from tests import scenes
+
+pytestmark = pytest.mark.gpu
+
+SPLIT_RTOL = 1e-6  # batch vs single-band split kernel, x max|single|
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = N.Context(0)
+    yield c
+    c.close()
+
+
+def _units(prep, solver, clock_mode=N.LPK_CLOCK_DEVICE_WALK, noise=True, seed=2026):
+    units = []
+    for w, (r, b) in enumerate(prep.work()):
+        d = prep.band_desc(r, b, seed, w)
+        d.solver = solver
+        d.clock_mode = clock_mode
+        if not noise:
+            d.noise_power_w = 0.0
+        units.append((d, prep.active(r, b), prep.n_samples(r, b)))
+    return units
+
+
+def _single(ctx, units, variant=0):
+    ctx.check(N.lib().lpk_ctx_set_split_variant(ctx.h, variant))
+    outs = []
+    for d, act, n in units:
+        out = np.zeros(max(n, 1), np.complex64)
+        a = np.ascontiguousarray(np.asarray(act, np.int32))
+        ctx.check(N.lib().lpk_band_chunk(ctx.h, C.byref(d), a.ctypes.data_as(N._I32) if a.size else None, a.size,
+                                         0, n, None, None, out.ctypes.data_as(N._CF), None))
+        outs.append(out[:n])
+    ctx.check(N.lib().lpk_ctx_set_split_variant(ctx.h, 0))
+    return outs
+
+
+def _rel(a, b):
+    scale = max(float(np.max(np.abs(b))) if b.size else 0.0, 1e-30)
+    return float(np.max(np.abs(a.astype(np.complex128) - b))) / scale if b.size else 0.0
+
+
+def _uneven_scene():
+    # 3 receivers with 1-3 bands of 48 kS/s - 4.096 MS/s, 24 C/A transmitters
+    return scenes.config_c2(duration_s=0.6, n_rx=3)
+
+
+def test_batch_reference_solver_is_bit_exact(ctx):
+    prep = P.Prepared(_uneven_scene(), ctx)
+    units = _units(prep, N.LPK_SOLVER_REFERENCE)
+    single = _single(ctx, units)
+    b = N.Batch(ctx, units, round_s=0.25)
+    got = b.render()
+    for u, (x, y) in enumerate(zip(got, single)):
+        assert x.shape == y.shape, u
+        assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), (u, _rel(x, y))
+    b.close()
+    prep.close()
+
+
+@pytest.mark.parametrize("variant", range(6))
+def test_batch_split_matches_single_band(ctx, variant):
+    prep = P.Prepared(scenes.config_c1(duration_s=1.5), ctx)
+    units = _units(prep, N.LPK_SOLVER_SPLIT)
+    prep2 = P.Prepared(_uneven_scene(), ctx)
+    units2 = _units(prep2, N.LPK_SOLVER_SPLIT)
+    for us in (units, units2):
+        single = _single(ctx, us, variant)
+        b = N.Batch(ctx, us, round_s=0.4)
+        b.set_config(variant)
+        got = b.render()
+        exact = 0
+        for u, (x, y) in enumerate(zip(got, single)):
+            assert x.shape == y.shape
+            assert _rel(x, y) <= SPLIT_RTOL, (variant, u, _rel(x, y))
+            exact += int(np.array_equal(x.view(np.uint32), y.view(np.uint32)))
+        print(f"variant {variant}: {exact}/{len(got)} units bit-identical to the single-band kernel")
+        b.close()
+    prep.close()
+    prep2.close()
+
+
+def test_batch_round_length_and_order_do_not_change_bits(ctx):
+    prep = P.Prepared(_uneven_scene(), ctx)
+    units = _units(prep, N.LPK_SOLVER_SPLIT)
+    ref = N.Batch(ctx, units, round_s=1.0).render()
+    b = N.Batch(ctx, units, round_s=0.13)
+    parts = [[None] * b.n_rounds for _ in units]
+    for r in reversed(range(b.n_rounds)):  # late rounds first: carries are completed on the way
+        b.run(r)
+        for u in range(len(units)):
+            n = b.extent(r, u)[1]
+            if n > 0:
+                parts[u][r] = b.output(u)[:n].copy()
+    for u in range(len(units)):
+        got = np.concatenate([p for p in parts[u] if p is not None])
+        assert np.array_equal(got.view(np.uint32), ref[u].view(np.uint32)), u
+    prep.close()
+
+
+def test_batch_deterministic_clock_and_no_walk(ctx):
+    prep = P.Prepared(scenes.config_c1(duration_s=1.0), ctx)
+    units = _units(prep, N.LPK_SOLVER_REFERENCE, clock_mode=N.LPK_CLOCK_DETERMINISTIC, noise=False)
+    single = _single(ctx, units)
+    got = N.Batch(ctx, units, round_s=0.3).render()
+    for x, y in zip(got, single):
+        assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+    prep.close()
+
+
+def test_batch_autotune_picks_a_measured_shape(ctx):
+    prep = P.Prepared(_uneven_scene(), ctx)
+    units = _units(prep, N.LPK_SOLVER_SPLIT)
+    b = N.Batch(ctx, units, round_s=0.3)
+    tab = b.autotune(rnd=1, reps=2)
+    measured = tab[tab > 0]
+    assert measured.size >= len(N.split_variants())
+    v, bps, max_bps = b.config()
+    assert 1 <= bps <= max_bps
+    assert abs(tab[v, 0 if bps == max_bps else 1] - measured.min()) < 1e-9
+    print("autotune ms per round (variant x [max, half] blocks/SM):\n", tab, "-> variant", v, "bps", bps)
+    single = _single(ctx, units, v)
+    got = b.render()
+    for x, y in zip(got, single):
+        assert _rel(x, y) <= SPLIT_RTOL
+    prep.close()
+
+
+def test_generate_scene_matches_generate_band(ctx):
+    sc = _uneven_scene()
+    prep = P.Prepared(sc, ctx)
+    work = prep.work()
+    batched = {w: [] for w in range(len(work))}
+    prep.generate_scene(2026, 0.2, lambda w, c: batched[w].append(c) and False, noise=True,
+                        device_clock=True, split=True)
+    for w, (r, b) in enumerate(work):
+        chunks = []
+        prep.generate_band(r, b, 2026, w, 1 << 18, lambda c: chunks.append(c) and False, noise=True,
+                           device_clock=True, split=True)
+        x = np.concatenate(batched[w])
+        y = np.concatenate(chunks)
+        assert x.shape == y.shape
+        assert _rel(x, y) <= SPLIT_RTOL, (w, _rel(x, y))
+    prep.close()
