@@ -60,6 +60,11 @@ def _args():
     p.add_argument("--solver", default="split", choices=["split", "reference"],
                    help="fan-out path timed for `value` (the plain FP64 kernel is timed beside split)")
     p.add_argument("--plain-steps", type=int, default=5, help="steps of the plain FP64 kernel (0: skip)")
+    p.add_argument("--path", default="batch", choices=["batch", "band"],
+                   help="batch: every (rx, band) unit per round in one graph-replayed persistent kernel; "
+                        "band: one launch pair per band chunk")
+    p.add_argument("--round-s", type=float, default=8.0, help="seconds of scene time per batch round")
+    p.add_argument("--no-autotune", action="store_true", help="keep the default split launch shape")
     return p.parse_args()
 
 
@@ -233,30 +238,71 @@ def run_ours(a):
     sc = _scene(a.duration)
     prep = P.Prepared(sc, ctx)
     per, total_band, total_txrx = _txrx_counts(prep)
+    solver = N.LPK_SOLVER_SPLIT if a.solver == "split" else N.LPK_SOLVER_REFERENCE
 
-    # device-resident outputs and per-band descriptors
+    # per-band descriptors and device-resident outputs
     bands = []
     for w, (r, b, n, k) in enumerate(per):
         d = prep.band_desc(r, b, seed, w)
         if d.clock_mode == N.LPK_CLOCK_HOST:
             d.clock_mode = N.LPK_CLOCK_DEVICE_WALK
-        d.solver = N.LPK_SOLVER_SPLIT if a.solver == "split" else N.LPK_SOLVER_REFERENCE
+        d.solver = solver
         act = prep.active(r, b)
-        out = torch.empty(2 * n, dtype=torch.float32, device=f"cuda:{local}")
-        bands.append((d, (C.c_int32 * max(len(act), 1))(*act), len(act), n, out))
-
-    def step():
-        for d, act, na, n, out in bands:
-            base = out.data_ptr()
-            for i0 in range(0, n, a.chunk):
-                m = min(a.chunk, n - i0)
-                N.check(L.lpk_band_chunk_device(ctx.h, C.byref(d), act, na, i0, m, None, None,
-                                                base + 8 * i0, None), ctx.h)
+        bands.append((d, act, n))
 
     def barrier():
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
+
+    def max_over_ranks(ms):
+        if dist is None:
+            return ms
+        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    band_out = [torch.empty(2 * n, dtype=torch.float32, device=f"cuda:{local}") for (_, _, n) in bands]
+    band_act = [(C.c_int32 * max(len(act), 1))(*act) for (_, act, _) in bands]
+
+    def band_step(which_solver):
+        for (d, act, n), cact, out in zip(bands, band_act, band_out):
+            d.solver = which_solver
+            base = out.data_ptr()
+            for i0 in range(0, n, a.chunk):
+                m = min(a.chunk, n - i0)
+                N.check(L.lpk_band_chunk_device(ctx.h, C.byref(d), cact, len(act), i0, m, None, None,
+                                                base + 8 * i0, None), ctx.h)
+
+    batch, tune = None, None
+    if a.path == "batch":
+        batch = N.Batch(ctx, [(d, act, n) for (d, act, n) in bands], a.round_s)
+        if not a.no_autotune and a.solver == "split":
+            tab = batch.autotune(rnd=batch.n_rounds // 2, reps=2)
+            v, bps, mx = batch.config()
+            tune = {"variant": v, "shape": dict(zip(("tile", "threads", "min_blocks"), N.split_variants()[v])),
+                    "blocks_per_sm": bps, "max_blocks_per_sm": mx,
+                    "ms_per_round": [[round(x, 4) for x in row] for row in tab.tolist()]}
+            ctx.check(L.lpk_ctx_set_split_variant(ctx.h, v))
+
+        def step():
+            ctx.check(L.lpk_batch_reset(batch.h))  # every step redoes the clock-walk carries
+            for r in range(batch.n_rounds):
+                ctx.check(L.lpk_batch_run(batch.h, r))
+    else:
+        def step():
+            band_step(solver)
+
+    def timed(fn, steps):
+        fn()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return max_over_ranks(e0.elapsed_time(e1))
 
     for _ in range(a.warmup):
         step()
@@ -266,6 +312,8 @@ def run_ours(a):
 
     N.check(L.lpk_profile_reset(ctx.h), ctx.h)
     N.check(L.lpk_profile_enable(ctx.h, 1), ctx.h)
+    step()  # graphs rebuilt with their profiling event nodes
+    N.check(L.lpk_profile_reset(ctx.h), ctx.h)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(local)
     barrier()
@@ -278,39 +326,40 @@ def run_ours(a):
     ev1.synchronize()
     clk = clocks.stop()
     barrier()
-    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
     fan_ms, fan_n, all_n = C.c_double(), C.c_int64(), C.c_int64()
     N.check(L.lpk_profile_read(ctx.h, C.byref(fan_ms), C.byref(fan_n), C.byref(all_n)), ctx.h)
     N.check(L.lpk_profile_enable(ctx.h, 0), ctx.h)
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     value = total_txrx * a.steps * ws / (ms * 1e-3)
 
-    # the plain all-FP64 kernel on the same scene (the metric's comparison)
-    plain = None
+    # comparisons on the same scene: the plain all-FP64 kernel (the metric's
+    # denominator), per band and batched, and the per-band split kernel
+    plain, others = None, {}
     if a.solver == "split" and a.plain_steps > 0:
-        for d, *_ in bands:
-            d.solver = N.LPK_SOLVER_REFERENCE
-        step()
-        barrier()
-        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        p0.record(stream)
-        for _ in range(a.plain_steps):
-            step()
-        p1.record(stream)
-        p1.synchronize()
-        pms = p0.elapsed_time(p1)
-        if dist is not None:
-            t = torch.tensor([pms], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            pms = float(t.item())
-        for d, *_ in bands:
-            d.solver = N.LPK_SOLVER_SPLIT
+        pms = timed(lambda: band_step(N.LPK_SOLVER_REFERENCE), a.plain_steps)
         plain = {"value": total_txrx * a.plain_steps * ws / (pms * 1e-3), "unit": UNIT,
                  "ms_per_step": pms / a.plain_steps, "steps": a.plain_steps,
-                 "kernel": "k_band_reference (reference semantics, all FP64)"}
+                 "kernel": "k_band_reference per band chunk (reference semantics, all FP64)"}
+        if a.path == "batch":
+            ref_batch = N.Batch(ctx, [(_clone(d, N.LPK_SOLVER_REFERENCE), act, n) for (d, act, n) in bands],
+                                a.round_s)
+
+            def ref_step():
+                ctx.check(L.lpk_batch_reset(ref_batch.h))
+                for r in range(ref_batch.n_rounds):
+                    ctx.check(L.lpk_batch_run(ref_batch.h, r))
+            bms = timed(ref_step, a.plain_steps)
+            others["plain_fp64_batched"] = {"value": total_txrx * a.plain_steps * ws / (bms * 1e-3),
+                                            "ms_per_step": bms / a.plain_steps,
+                                            "kernel": "k_batch_fanout, every sample on the exact FP64 path"}
+            if others["plain_fp64_batched"]["value"] > plain["value"]:
+                plain, others["plain_fp64_per_band"] = dict(others.pop("plain_fp64_batched"), unit=UNIT,
+                                                            steps=a.plain_steps), plain
+            ref_batch.close()
+            sms = timed(lambda: band_step(N.LPK_SOLVER_SPLIT), a.plain_steps)
+            others["split_per_band"] = {"value": total_txrx * a.plain_steps * ws / (sms * 1e-3),
+                                        "ms_per_step": sms / a.plain_steps,
+                                        "kernel": "k_split_anchor + k_band_split per band chunk"}
 
     # roofline of the dominant kernel (the fan-out), from its own events
     avg_launch_ms = fan_ms.value / max(fan_n.value, 1)
@@ -325,38 +374,32 @@ def run_ours(a):
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     hbm_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
-    traffic = _traffic_from_profile(band_per_launch, a.solver)
+    traffic = _traffic_from_profile(band_per_launch, f"{a.solver}_{a.path}")
     achieved_gbs = BYTES_PER_BAND_SAMPLE * band_per_launch / (avg_launch_ms * 1e-3) / 1e9
 
-    # e2e through the host-level C ABI, host buffers
+    # e2e through the host-level C ABI with host buffers: scene preparation
+    # (tables built and uploaded) and every chunk copied to pinned host memory
     e2e = None
     if not a.no_e2e:
-        host = np.empty(2 * max(n for _, _, n, _ in per), dtype=np.float32)
-        hptr = host.ctypes.data
-        pos = [0]
+        seen = [0]
 
-        def sink(_u, ptr, n):
-            C.memmove(hptr + 8 * pos[0], ptr, 8 * n)
-            pos[0] += n
+        def sink(_u, w, ptr, n):
+            seen[0] += n  # the chunk sits in pinned host memory; a writer would take it from here
             return 0
 
-        cb = N.SINK_FN(sink)
+        cb = N.UNIT_SINK_FN(sink)
         h2d = 0
         for i in range(len(sc.transmitters)):
             td = N.TxDesc()
             N.check(L.lpk_scene_tx_desc(prep.h, i, C.byref(td)))
             h2d += 24 * td.grid_n + td.n_sym * (8 if td.sig_kind == 3 else 1) + (1023 if td.sig_kind == 4 else 0)
+        flags = N.LPK_NOISE_ON | N.LPK_GEN_DEVICE_CLOCK | (N.LPK_GEN_SPLIT if a.solver == "split" else 0)
 
         def e2e_step():
             p2 = P.Prepared(sc, ctx)
-            for w, (r, b) in enumerate(p2.work()):
-                pos[0] = 0
-                res = N.BandResult()
-                N.check(L.lpk_generate_band(p2.h, r, b, seed, w, P.DEFAULT_CHUNK_SAMPLES,
-                                            N.LPK_NOISE_ON | N.LPK_GEN_DEVICE_CLOCK
-                                            | (N.LPK_GEN_SPLIT if a.solver == "split" else 0),
-                                            cb, None, C.byref(res)),
-                        ctx.h)
+            seen[0] = 0
+            N.check(L.lpk_generate_scene(p2.h, seed, a.round_s, flags, cb, None), ctx.h)
+            assert seen[0] == total_band
             p2.close()
 
         e2e_step()
@@ -369,41 +412,47 @@ def run_ours(a):
         e1.record(stream)
         e1.synchronize()
         wall = time.perf_counter() - t0
-        ems = max(e0.elapsed_time(e1), 1e3 * wall)
-        if dist is not None:
-            t = torch.tensor([ems], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
+        ems = max_over_ranks(max(e0.elapsed_time(e1), 1e3 * wall))
         e2e = {"value": total_txrx * a.e2e_steps * ws / (ems * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(BYTES_PER_BAND_SAMPLE * total_band),
-               "path": "lpk_scene_prepare + lpk_generate_band (C ABI) into host memory, 2^20-sample chunks"}
+               "ms_per_step": ems / a.e2e_steps,
+               "path": f"lpk_scene_prepare + lpk_generate_scene (C ABI): batched rounds of {a.round_s} s, "
+                       "outputs double-buffered into pinned host memory on a copy stream"}
 
     base = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         base, _ = cpu_baseline(a.duration, a.cpu_seconds)
 
+    if batch is not None:
+        batch.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return 0
+    kernel = ("k_batch_fanout (persistent, all units)" if a.path == "batch" else
+              ("k_band_split" if a.solver == "split" else "k_band_reference"))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded scene, no dataset)",
         "config": {"workload": WORKLOAD, "duration_s": a.duration, "tx_rx_samples_per_step_per_gpu": total_txrx,
-                   "band_samples_per_step_per_gpu": total_band, "chunk_samples": a.chunk,
-                   "solver": ("split precision: FP64 anchors per 1024-sample tile (reference 2-iteration solve), "
+                   "band_samples_per_step_per_gpu": total_band,
+                   "path": (f"batched: rounds of {a.round_s} s, one CUDA graph per round (walk scan + carries "
+                            "beside the anchor fits, then one persistent fan-out over every unit's tiles)")
+                   if a.path == "batch" else f"per band, chunks of {a.chunk} samples",
+                   "launch_shape": tune,
+                   "solver": ("split precision: FP64 anchors per tile (reference 2-iteration solve), "
                               "quadratic delay per sample, FP64 phase reduction, FP32 sin/cos and MAC; "
                               "indices bit-exact via guard-band fallback") if a.solver == "split" else
                              "reference semantics: 2 fixed-point iterations from t-70 ms, all FP64",
-                   "clock": "white-FM walk generated on the device", "noise": "AWGN on",
+                   "clock": "white-FM walk generated on the device, carries recomputed every step",
+                   "noise": "AWGN on",
                    "parallelism": f"{ws} GPU(s), one scene replica per GPU",
                    "l2": "output (1.97 GB/step) is larger than L2; scene tables (~3 MB) are L2-resident by design"},
         "roofline": {"bound": "fp64", "achieved": achieved_tf, "peak": peak_fp64.value, "unit": "TFLOP/s",
                      "frac": achieved_tf / peak_fp64.value if peak_fp64.value else None,
-                     "traffic": traffic,
-                     "kernel": "k_split_anchor + k_band_split" if a.solver == "split" else "k_band_reference",
+                     "traffic": traffic, "kernel": kernel,
                      "basis": f"{FLOP_PER_SAMPLE} FP64-equivalent flop per tx·rx sample x {txrx_per_launch:.4g} "
                               f"tx·rx samples per launch / {avg_launch_ms:.3f} ms average launch (CUDA events "
                               "on the launching stream); peak = FP64 DFMA probe measured in this run",
@@ -411,13 +460,22 @@ def run_ours(a):
                              "frac": achieved_gbs / hbm_peak, "peak_source": hbm_src,
                              "algorithmic_bytes_per_launch": BYTES_PER_BAND_SAMPLE * band_per_launch}},
         "e2e": e2e, "gpu_launches": int(all_n.value), "clocks": clk,
-        "plain_fp64": plain,
+        "plain_fp64": plain, "other_paths": others or None,
         "speedup_vs_plain_fp64": (value / plain["value"]) if plain else None,
     }
     if base is not None:
         line["cpu_baseline"] = base
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _clone(d, solver):
+    import ctypes as C2
+    from lipika_b200 import native as N
+    e = N.BandDesc()
+    C2.memmove(C2.byref(e), C2.byref(d), C2.sizeof(N.BandDesc))
+    e.solver = solver
+    return e
 
 
 def main():

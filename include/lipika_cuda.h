@@ -282,6 +282,17 @@ lpk_status lpk_batch_run(lpk_batch *b, int64_t round);
 lpk_status lpk_batch_output(lpk_batch *b, int32_t unit, const lpk_cf32 **d_out);
 /* Wait for the last round and copy unit `unit`'s output to host memory. */
 lpk_status lpk_batch_copy_out(lpk_batch *b, int32_t unit, lpk_cf32 *host, int64_t cap);
+/* Forget the clock-walk carries computed so far, so the next rounds redo
+ * all the walk work a fresh batch would (outputs are unchanged). */
+lpk_status lpk_batch_reset(lpk_batch *b);
+/* Sink of lpk_batch_render / lpk_generate_scene: one unit's chunk, in
+ * order; return 0 to continue, 1 to stop that unit, negative to abort. */
+typedef int32_t (*lpk_unit_sink_fn)(void *user, int32_t unit, const lpk_cf32 *chunk, int64_t n);
+/* Every round in order with the outputs double-buffered: while round k
+ * renders, round k-1's outputs are copied to pinned host staging on a
+ * second stream and handed to sink(user, unit, chunk, n) (the chunk points
+ * into the staging; valid during the call). */
+lpk_status lpk_batch_render(lpk_batch *b, lpk_unit_sink_fn sink, void *user);
 /* Launch configuration: split shape and persistent blocks per SM (0 = the
  * most that fit). */
 lpk_status lpk_batch_set_config(lpk_batch *b, int32_t variant, int32_t blocks_per_sm);
@@ -358,13 +369,12 @@ lpk_status lpk_generate_band_to_file(lpk_scene *s, int32_t r_idx, int32_t b_idx,
 
 /* Every work unit of the scene through one lpk_batch (run_scene_in_memory /
  * run_scene_to_dir, src/pipeline.rs:460-536, with the per-unit
- * generate_band calls fused): rounds of round_s seconds, each unit's chunk
- * handed to sink_unit(user, work_idx, chunk, n) in order. Work units whose
+ * generate_band calls fused): rounds of round_s seconds, each work unit's
+ * chunk handed to sink(user, work_idx, chunk, n) in order. Work units whose
  * receiver moves or whose clock has flicker are rendered by
  * lpk_generate_band instead, after the batch. Flags as lpk_generate_band,
  * plus LPK_GEN_AUTOTUNE (tune the launch shape on the middle round first). */
 enum { LPK_GEN_AUTOTUNE = 8 };
-typedef int32_t (*lpk_unit_sink_fn)(void *user, int32_t work_idx, const lpk_cf32 *chunk, int64_t n);
 lpk_status lpk_generate_scene(lpk_scene *s, uint64_t seed_base, double round_s, int32_t flags,
                               lpk_unit_sink_fn sink, void *user);
 

@@ -164,39 +164,43 @@ lpk_status prepare_walk(lpk_ctx *c, const lpk_band_desc *d, int64_t i0, int64_t 
         w->fm = d->clock_master_rate_hz;
         w->sigma = sigma;
     }
-    const int64_t need = kB / kWalkBlock;  // carry(need) must be known
+    const int64_t bA = kA / kWalkBlock, need = kB / kWalkBlock;  // carries of blocks [bA, need]
     if (need + 1 > w->cap) {
         int64_t cap = w->cap ? w->cap : 1024;
         while (cap < need + 1) cap *= 2;
-        double *tot = nullptr, *car = nullptr;
+        double *tot = nullptr, *car = nullptr, *gs = nullptr;
         cudaError_t e = cudaMalloc(&tot, sizeof(double) * (size_t)cap);
         if (e == cudaSuccess) e = cudaMalloc(&car, sizeof(double) * (size_t)(cap + 1));
+        if (e == cudaSuccess) e = cudaMalloc(&gs, sizeof(double) * (size_t)(cap / kGroupBlocks + 1));
         if (e != cudaSuccess) {
             if (tot) cudaFree(tot);
+            if (car) cudaFree(car);
             return fail(c, LPK_ENOMEM, "clock walk carry allocation failed");
         }
-        if (w->nb_done > 0) {
+        if (w->nb_done > 0)
             cudaMemcpyAsync(tot, w->d_tot, sizeof(double) * (size_t)w->nb_done, cudaMemcpyDeviceToDevice, c->stream);
-            cudaMemcpyAsync(car, w->d_carry, sizeof(double) * (size_t)(w->nb_done + 1), cudaMemcpyDeviceToDevice,
-                            c->stream);
-        }
+        if (w->g_known > 0)
+            cudaMemcpyAsync(gs, w->d_gsum, sizeof(double) * (size_t)w->g_known, cudaMemcpyDeviceToDevice, c->stream);
         cudaStreamSynchronize(c->stream);
         if (w->d_tot) cudaFree(w->d_tot);
         if (w->d_carry) cudaFree(w->d_carry);
+        if (w->d_gsum) cudaFree(w->d_gsum);
         w->d_tot = tot;
         w->d_carry = car;
+        w->d_gsum = gs;
         w->cap = cap;
     }
     cudaError_t e = cudaSuccess;
-    if (need > w->nb_done || (need == 0 && w->nb_done == 0)) {
-        if (w->nb_done == 0) e = cudaMemsetAsync(w->d_carry, 0, sizeof(double), c->stream);
-        if (e == cudaSuccess && need > w->nb_done) {
-            e = launch_walk_totals(w->seed, w->sigma, w->nb_done, need, w->d_tot, w->d_carry, c->stream);
-            c->launches += 2;
-        }
+    if (need > w->nb_done) {
+        e = launch_walk_totals(w->seed, w->sigma, w->nb_done, need, w->d_tot, c->stream);
+        c->launches += 1;
         if (e != cudaSuccess) return cuda_fail(c, e, "clock walk totals");
-        if (need > w->nb_done) w->nb_done = need;
+        w->nb_done = need;
     }
+    e = launch_walk_carries(w->d_tot, w->d_gsum, w->g_known, bA, need, w->d_carry, c->stream);
+    c->launches += 1;
+    if (e != cudaSuccess) return cuda_fail(c, e, "clock walk carries");
+    if (need / kGroupBlocks > w->g_known) w->g_known = need / kGroupBlocks;
     e = launch_walk_materialize(w->seed, w->sigma, w->d_carry, kA, kB, d_eps, c->stream);
     c->launches += 1;
     if (e != cudaSuccess) return cuda_fail(c, e, "clock walk materialisation");
@@ -215,6 +219,20 @@ void prof_begin(lpk_ctx *c) {
         c->prof_events.push_back({a, b});
     }
     cudaEventRecord(c->prof_events[c->prof_used].first, c->stream);
+}
+
+bool prof_take(lpk_ctx *c, cudaEvent_t &a, cudaEvent_t &b) {
+    if (!c->profiling) return false;
+    if (c->prof_used == c->prof_events.size()) {
+        cudaEvent_t x, y;
+        if (cudaEventCreate(&x) != cudaSuccess) return false;
+        if (cudaEventCreate(&y) != cudaSuccess) { cudaEventDestroy(x); return false; }
+        c->prof_events.push_back({x, y});
+    }
+    a = c->prof_events[c->prof_used].first;
+    b = c->prof_events[c->prof_used].second;
+    ++c->prof_used;
+    return true;
 }
 
 void prof_end(lpk_ctx *c) {
@@ -347,6 +365,7 @@ void lpk_ctx_destroy(lpk_ctx *c) {
     for (auto &w : c->walks) {
         if (w.d_tot) cudaFree(w.d_tot);
         if (w.d_carry) cudaFree(w.d_carry);
+        if (w.d_gsum) cudaFree(w.d_gsum);
     }
     for (auto &p : c->prof_events) {
         cudaEventDestroy(p.first);

@@ -30,7 +30,8 @@ struct BatchUnit {
     int32_t act_off, n_active;
     int32_t walk;        // index into the walk table, -1 without a device walk
     int32_t exact_only;  // reference-exact path for every sample
-    float2 *out;         // round output buffer (capacity: the unit's round length)
+    float2 *out[2];      // round output buffers (capacity: the unit's round length),
+                         // alternating between rounds so one can be read while the next renders
 };
 
 // One receiver clock walk: the scan blocks' totals and carries over the
@@ -40,7 +41,8 @@ struct DevWalk {
     double sigma;
     double *partial;  // P_b(k) for k in [bA·kWalkBlock, (bB+1)·kWalkBlock)
     double *totals;   // per scan block
-    double *carry;    // carry[b] = Σ totals[0..b-1]
+    double *gsum;     // per carry group of kGroupBlocks scan blocks
+    double *carry;    // carry[b] = Σ totals[0..b-1] in the fixed order of lpk_walk.cuh
 };
 
 // Per round (copied to the device by the graph's first node).
@@ -52,11 +54,11 @@ struct RoundUnit {
 };
 struct RoundWalk {
     int64_t b_lo, bA, bB;   // blocks [b_lo, bB] are scanned, P_b stored for [bA, bB]
-    int64_t carry_from;     // carries [carry_from + 1, bB] are added
+    int64_t g_known;        // groups whose sums are stored before the round
 };
 struct RoundDesc {
     int64_t total_tiles, total_recs, total_walk_blocks;
-    int32_t n_slots, n_walks, tile, pad;
+    int32_t n_slots, n_walks, tile, parity;  // parity: which output buffer the round writes
     int64_t wb_off[kMaxWalks + 1];  // prefix of scanned blocks per walk
     RoundWalk w[kMaxWalks];
     RoundUnit s[kMaxUnits];         // schedule slots, most work first
@@ -103,25 +105,19 @@ k_batch_walk(const DevWalk *__restrict__ walks, const RoundDesc *__restrict__ rd
     }
 }
 
-// carry(b + 1) = carry(b) ⊕ total(b) in block order, one warp (block) per
-// walk: 32 totals are loaded at once, the sum stays sequential.
-__global__ void __launch_bounds__(32) k_batch_carry(const DevWalk *__restrict__ walks,
-                                                    const RoundDesc *__restrict__ rd) {
-    const int w = (int)blockIdx.x, lane = (int)threadIdx.x;
+// Carries of the round's blocks [bA, bB] of every walk: blockIdx.y is the
+// walk, blocks stride over its carry groups (lpk_walk.cuh).
+__global__ void __launch_bounds__(kGroupThreads)
+k_batch_carry(const DevWalk *__restrict__ walks, const RoundDesc *__restrict__ rd) {
+    __shared__ double sh[65];
+    const int w = (int)blockIdx.y;
     if (w >= rd->n_walks) return;
     const RoundWalk rw = rd->w[w];
+    if (rw.bB < rw.bA) return;
     const DevWalk dw = walks[w];
-    double c = dw.carry[rw.carry_from];
-    for (int64_t b0 = rw.carry_from; b0 < rw.bB; b0 += 32) {
-        const int64_t nb = rw.bB - b0 < 32 ? rw.bB - b0 : 32;
-        const double t = lane < nb ? dw.totals[b0 + lane] : 0.0;
-        double mine = 0.0;
-        for (int j = 0; j < (int)nb; ++j) {
-            c = __dadd_rn(c, __shfl_sync(0xffffffffu, t, j));
-            if (lane == j) mine = c;
-        }
-        if (lane < nb) dw.carry[b0 + lane + 1] = mine;
-    }
+    const int64_t gA = rw.bA / kGroupBlocks, gB = rw.bB / kGroupBlocks;
+    for (int64_t g = gA + blockIdx.x; g <= gB; g += gridDim.x)
+        walk_group_carries(dw.totals, dw.gsum, rw.g_known, rw.bA, rw.bB, g, g == gA, dw.carry, sh);
 }
 
 // Anchor fits of every (slot, tile, transmitter) of the round.
@@ -188,7 +184,7 @@ k_batch_fanout(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ 
         cur = ru.unit;
         __syncthreads();
         const int64_t first = (ru.t0 + local) * TILE - ru.i0;
-        split_tile<TILE / THREADS, THREADS, false>(*sb, stx, srec, bu.n_active, first, bu.out, nullptr, nullptr,
+        split_tile<TILE / THREADS, THREADS, false>(*sb, stx, srec, bu.n_active, first, bu.out[rd->parity], nullptr, nullptr,
                                                    nullptr);
         __syncthreads();  // the next stage overwrites the shared tiles
     }
@@ -224,7 +220,8 @@ struct UnitHost {
 struct WalkHost {
     uint64_t seed = 0;
     double fm = 0.0, sigma = 0.0;
-    int64_t carry_done = 0;  // carry[b] is known for b <= carry_done
+    int64_t totals_done = 0;  // totals of blocks below this are known
+    int64_t g_known = 0;      // sums of groups below this are stored
     int64_t partial_cap = 0;
 };
 
@@ -240,16 +237,26 @@ struct lpk_batch {
     DevWalk *d_walks = nullptr;
     RoundDesc *d_round = nullptr;
     RoundDesc *h_round[2] = {nullptr, nullptr};  // pinned, alternating between rounds
-    cudaEvent_t done[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};       // round of parity p finished
+    cudaEvent_t copied[2] = {nullptr, nullptr};     // output copies of parity p finished
+    cudaStream_t side = nullptr;                    // graph branch: anchors beside the walk scan
+    cudaStream_t copy = nullptr;                    // device-to-host copies of finished rounds
+    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaEvent_t mark[2] = {nullptr, nullptr};       // placeholders of the profiling event nodes
     AnchorRec *d_recs = nullptr;
     unsigned long long *d_counter = nullptr;
     int64_t recs_cap = 0;
     int64_t n_rounds = 0;
     int32_t max_active = 0;
     int variant = 0, bps = 0, max_bps = 0, walk_grid = 0, anchor_grid = 0;
+    cudaGraph_t graph_src[2] = {nullptr, nullptr};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    int parity = 0;
+    bool graph_prof[2] = {false, false};            // built with event nodes around the fan-out
+    cudaGraphNode_t prof_node[2][2] = {};
+    int parity = 0, last_parity = 0;
     int64_t last_round = -1;
+    std::vector<lpk_cf32 *> staging[2];             // pinned host copies (lpk_batch_render), in the
+                                                    // context's pinned pool
 };
 
 namespace {
@@ -321,17 +328,19 @@ void plan_round(lpk_batch *b, int64_t round, int tile, RoundDesc &rd, bool commi
         if (kB[w] < 0) {  // no unit of this walk renders in this round
             rw.b_lo = rw.bA = 0;
             rw.bB = -1;
-            rw.carry_from = 0;
+            rw.g_known = wh.g_known;
             continue;
         }
         rw.bA = kA[w] / kWalkBlock;
         rw.bB = kB[w] / kWalkBlock;
-        rw.b_lo = std::min(rw.bA, wh.carry_done);
-        rw.carry_from = wh.carry_done;
-        if (rw.carry_from > rw.bB) rw.carry_from = rw.bB;  // nothing new to carry
+        rw.b_lo = std::min(rw.bA, wh.totals_done);
+        rw.g_known = wh.g_known;
         wb += rw.bB - rw.b_lo + 1;
         partial_blocks = std::max(partial_blocks, rw.bB - rw.bA + 1);
-        if (commit) wh.carry_done = std::max(wh.carry_done, rw.bB);
+        if (commit) {
+            wh.totals_done = std::max(wh.totals_done, rw.bB + 1);
+            wh.g_known = std::max(wh.g_known, rw.bB / kGroupBlocks);
+        }
     }
     rd.wb_off[b->walks.size()] = wb;
     rd.total_walk_blocks = wb;
@@ -340,16 +349,19 @@ void plan_round(lpk_batch *b, int64_t round, int tile, RoundDesc &rd, bool commi
 }
 
 void drop_graphs(lpk_batch *b) {
-    for (auto &g : b->graph)
-        if (g) {
-            cudaGraphExecDestroy(g);
-            g = nullptr;
-        }
+    for (int p = 0; p < 2; ++p) {
+        if (b->graph[p]) cudaGraphExecDestroy(b->graph[p]);
+        if (b->graph_src[p]) cudaGraphDestroy(b->graph_src[p]);
+        b->graph[p] = nullptr;
+        b->graph_src[p] = nullptr;
+    }
 }
 
-// Capture the round graph (descriptor copy from h_round[p], walk scan,
-// carries, anchors, counter reset, persistent fan-out) for the current
-// launch configuration.
+// Capture the round graph for the current launch configuration: the copy of
+// descriptor h_round[p]; then, in parallel, the anchor fits (side branch)
+// and the walk scan with its carries; then the counter reset and the
+// persistent fan-out. With profiling on, two event-record nodes bracket the
+// fan-out; each launch points them at a fresh event pair of the context.
 lpk_status build_graph(lpk_batch *b, int p) {
     lpk_ctx *c = b->ctx;
     const FanoutShape &sh = kFanout[b->variant];
@@ -358,31 +370,59 @@ lpk_status build_graph(lpk_batch *b, int p) {
     if (e != cudaSuccess) return cuda_fail(c, e, "batch fan-out shared memory");
     int dev_sms = 0;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
+    const bool prof = c->profiling;
     cudaGraph_t g = nullptr;
     e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_fail(c, e, "batch graph capture");
     cudaMemcpyAsync(b->d_round, b->h_round[p], sizeof(RoundDesc), cudaMemcpyHostToDevice, c->stream);
+    cudaEventRecord(b->fork, c->stream);
+    cudaStreamWaitEvent(b->side, b->fork, 0);
+    k_batch_anchor<<<b->anchor_grid, 128, 0, b->side>>>(b->d_bands, b->d_units, c->d_tx, b->d_act, b->d_round,
+                                                        b->d_recs);
+    cudaEventRecord(b->join, b->side);
     if (!b->walks.empty()) {
         k_batch_walk<<<b->walk_grid, kWalkThreads, 0, c->stream>>>(b->d_walks, b->d_round);
-        k_batch_carry<<<(unsigned)b->walks.size(), 32, 0, c->stream>>>(b->d_walks, b->d_round);
+        k_batch_carry<<<dim3(8, (unsigned)b->walks.size()), kGroupThreads, 0, c->stream>>>(b->d_walks, b->d_round);
     }
-    k_batch_anchor<<<b->anchor_grid, 128, 0, c->stream>>>(b->d_bands, b->d_units, c->d_tx, b->d_act, b->d_round,
-                                                          b->d_recs);
+    cudaStreamWaitEvent(c->stream, b->join, 0);
     cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), c->stream);
+    if (prof) cudaEventRecordWithFlags(b->mark[0], c->stream, cudaEventRecordExternal);
     sh.kern<<<(unsigned)(dev_sms * b->bps), sh.threads, smem, c->stream>>>(
         b->d_bands, b->d_units, c->d_tx, b->d_act, b->d_walks, b->d_round, b->d_recs, b->d_counter, b->max_active);
+    if (prof) cudaEventRecordWithFlags(b->mark[1], c->stream, cudaEventRecordExternal);
     cudaError_t le = cudaGetLastError();
     e = cudaStreamEndCapture(c->stream, &g);
     if (le != cudaSuccess || e != cudaSuccess) {
         if (g) cudaGraphDestroy(g);
         return cuda_fail(c, le != cudaSuccess ? le : e, "batch graph capture");
     }
+    b->graph_prof[p] = prof;
+    if (prof) {  // find the two event-record nodes by their placeholder events
+        size_t n = 0;
+        cudaGraphGetNodes(g, nullptr, &n);
+        std::vector<cudaGraphNode_t> nodes(n);
+        cudaGraphGetNodes(g, nodes.data(), &n);
+        b->prof_node[p][0] = b->prof_node[p][1] = nullptr;
+        for (cudaGraphNode_t nd : nodes) {
+            cudaGraphNodeType t;
+            cudaEvent_t ev = nullptr;
+            if (cudaGraphNodeGetType(nd, &t) != cudaSuccess || t != cudaGraphNodeTypeEventRecord) continue;
+            if (cudaGraphEventRecordNodeGetEvent(nd, &ev) != cudaSuccess) continue;
+            for (int k = 0; k < 2; ++k)
+                if (ev == b->mark[k]) b->prof_node[p][k] = nd;
+        }
+        if (!b->prof_node[p][0] || !b->prof_node[p][1]) {
+            cudaGraphDestroy(g);
+            return fail(c, LPK_ECUDA, "profiling nodes missing from the round graph");
+        }
+    }
     e = cudaGraphInstantiate(&b->graph[p], g, 0);
-    cudaGraphDestroy(g);
     if (e != cudaSuccess) {
+        cudaGraphDestroy(g);
         b->graph[p] = nullptr;
         return cuda_fail(c, e, "batch graph instantiate");
     }
+    b->graph_src[p] = g;
     return LPK_OK;
 }
 
@@ -434,12 +474,18 @@ void lpk_batch_destroy(lpk_batch *b) {
         cudaSetDevice(b->ctx->device);
         cudaStreamSynchronize(b->ctx->stream);
     }
+    if (b->copy) cudaStreamSynchronize(b->copy);
     drop_graphs(b);
     for (void *p : b->allocs) cudaFree(p);
     for (auto &h : b->h_round)
         if (h) cudaFreeHost(h);
-    for (auto &ev : b->done)
+    for (int i = 0; i < 2; ++i)
+        for (cudaEvent_t ev : {b->done[i], b->copied[i], b->mark[i]})
+            if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : {b->fork, b->join})
         if (ev) cudaEventDestroy(ev);
+    for (cudaStream_t st : {b->side, b->copy})
+        if (st) cudaStreamDestroy(st);
     delete b;
 }
 
@@ -519,7 +565,7 @@ lpk_status lpk_batch_create(lpk_ctx *c, const lpk_work_unit *wu, int32_t n_units
     }
     std::vector<int64_t> total_blocks(b->walks.size(), 1);
     for (size_t w = 0; w < b->walks.size(); ++w) {
-        total_blocks[w] = b->walks[w].carry_done + 2;
+        total_blocks[w] = b->walks[w].totals_done + 2;
         saved[w].partial_cap = b->walks[w].partial_cap;
     }
     b->walks = saved;  // carry bookkeeping restarts at block 0
@@ -534,10 +580,11 @@ lpk_status lpk_batch_create(lpk_ctx *c, const lpk_work_unit *wu, int32_t n_units
     if (!st) st = batch_alloc(b, &p, sizeof(unsigned long long)), b->d_counter = (unsigned long long *)p;
     if (!st) st = batch_alloc(b, &p, sizeof(DevWalk) * std::max<size_t>(1, b->walks.size())),
              b->d_walks = (DevWalk *)p;
-    for (int u = 0; u < n_units && !st; ++u) {
-        st = batch_alloc(b, &p, sizeof(float2) * (size_t)b->units[u].round_len);
-        b->h_units[u].out = (float2 *)p;
-    }
+    for (int u = 0; u < n_units && !st; ++u)
+        for (int k = 0; k < 2 && !st; ++k) {
+            st = batch_alloc(b, &p, sizeof(float2) * (size_t)b->units[u].round_len);
+            b->h_units[u].out[k] = (float2 *)p;
+        }
     std::vector<DevWalk> h_walks(b->walks.size());
     for (size_t w = 0; w < b->walks.size() && !st; ++w) {
         h_walks[w].seed = b->walks[w].seed;
@@ -546,15 +593,22 @@ lpk_status lpk_batch_create(lpk_ctx *c, const lpk_work_unit *wu, int32_t n_units
         h_walks[w].partial = (double *)p;
         if (!st) st = batch_alloc(b, &p, sizeof(double) * (size_t)total_blocks[w]), h_walks[w].totals = (double *)p;
         if (!st) st = batch_alloc(b, &p, sizeof(double) * (size_t)(total_blocks[w] + 1)), h_walks[w].carry = (double *)p;
-        if (!st && cudaMemsetAsync(h_walks[w].carry, 0, sizeof(double), c->stream) != cudaSuccess)
-            st = fail(c, LPK_ECUDA, "walk carry reset failed");
+        if (!st) st = batch_alloc(b, &p, sizeof(double) * (size_t)(total_blocks[w] / kGroupBlocks + 1)),
+                 h_walks[w].gsum = (double *)p;
     }
     for (int i = 0; i < 2 && !st; ++i) {
         if (cudaHostAlloc((void **)&b->h_round[i], sizeof(RoundDesc), cudaHostAllocDefault) != cudaSuccess)
             st = fail(c, LPK_ENOMEM, "pinned round descriptor allocation failed");
-        else if (cudaEventCreateWithFlags(&b->done[i], cudaEventDisableTiming) != cudaSuccess)
+        else if (cudaEventCreateWithFlags(&b->done[i], cudaEventDisableTiming) != cudaSuccess ||
+                 cudaEventCreateWithFlags(&b->copied[i], cudaEventDisableTiming) != cudaSuccess ||
+                 cudaEventCreate(&b->mark[i]) != cudaSuccess)
             st = fail(c, LPK_ECUDA, "event creation failed");
     }
+    if (!st && (cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaStreamCreateWithFlags(&b->copy, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess))
+        st = fail(c, LPK_ECUDA, "stream or event creation failed");
     if (!st) {
         cudaError_t e = cudaMemcpyAsync(b->d_bands, h_bands.data(), sizeof(DevBand) * (size_t)n_units,
                                         cudaMemcpyHostToDevice, c->stream);
@@ -604,20 +658,45 @@ lpk_status lpk_batch_run(lpk_batch *b, int64_t round) {
     if (round < 0 || round >= b->n_rounds) return fail(c, LPK_EINVAL, "round out of range");
     cudaSetDevice(c->device);
     const int p = b->parity;
-    // the descriptor buffer p was last read by the round launched two calls ago
+    // descriptor buffer p was last read by the round launched two calls ago
     cudaError_t e = cudaEventSynchronize(b->done[p]);
     if (e != cudaSuccess) return cuda_fail(c, e, "batch round wait");
     int tile = 0;
     split_variant_info(b->variant, &tile, nullptr, nullptr);
     plan_round(b, round, tile, *b->h_round[p], true, nullptr, nullptr);
+    b->h_round[p]->parity = p;
     lpk_status st = LPK_OK;
+    if (b->graph[p] && b->graph_prof[p] != c->profiling) {
+        cudaGraphExecDestroy(b->graph[p]);
+        cudaGraphDestroy(b->graph_src[p]);
+        b->graph[p] = nullptr;
+        b->graph_src[p] = nullptr;
+    }
     if (!b->graph[p] && (st = build_graph(b, p))) return st;
-    e = cudaGraphLaunch(b->graph[p], c->stream);
+    cudaEvent_t ea, eb;
+    if (b->graph_prof[p] && prof_take(c, ea, eb)) {
+        e = cudaGraphExecEventRecordNodeSetEvent(b->graph[p], b->prof_node[p][0], ea);
+        if (e == cudaSuccess) e = cudaGraphExecEventRecordNodeSetEvent(b->graph[p], b->prof_node[p][1], eb);
+        if (e != cudaSuccess) return cuda_fail(c, e, "profiling event nodes");
+    }
+    // the output buffers of parity p may still be being copied out (round - 2)
+    e = cudaStreamWaitEvent(c->stream, b->copied[p], 0);
+    if (e == cudaSuccess) e = cudaGraphLaunch(b->graph[p], c->stream);
     if (e == cudaSuccess) e = cudaEventRecord(b->done[p], c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "batch graph launch");
     c->launches += 2 + (b->walks.empty() ? 0 : 2);
+    b->last_parity = p;
     b->parity ^= 1;
     b->last_round = round;
+    return LPK_OK;
+}
+
+lpk_status lpk_batch_reset(lpk_batch *b) {
+    if (!b) return fail(nullptr, LPK_EINVAL, "batch is NULL");
+    for (auto &w : b->walks) {
+        w.totals_done = 0;
+        w.g_known = 0;
+    }
     return LPK_OK;
 }
 
@@ -625,7 +704,7 @@ lpk_status lpk_batch_output(lpk_batch *b, int32_t unit, const lpk_cf32 **d_out) 
     if (!b) return fail(nullptr, LPK_EINVAL, "batch is NULL");
     if (unit < 0 || unit >= (int32_t)b->units.size()) return fail(b->ctx, LPK_EINVAL, "unit out of range");
     if (!d_out) return fail(b->ctx, LPK_EINVAL, "d_out is NULL");
-    *d_out = (const lpk_cf32 *)b->h_units[unit].out;
+    *d_out = (const lpk_cf32 *)b->h_units[unit].out[b->last_parity];
     return LPK_OK;
 }
 
@@ -638,12 +717,68 @@ lpk_status lpk_batch_copy_out(lpk_batch *b, int32_t unit, lpk_cf32 *host, int64_
     unit_extent(b, b->last_round, unit, i0, n);
     if (n > 0 && (!host || cap < n)) return fail(c, LPK_EINVAL, "host buffer is NULL or too small");
     cudaSetDevice(c->device);
-    cudaError_t e = n > 0 ? cudaMemcpyAsync(host, b->h_units[unit].out, sizeof(lpk_cf32) * (size_t)n,
+    cudaError_t e = n > 0 ? cudaMemcpyAsync(host, b->h_units[unit].out[b->last_parity], sizeof(lpk_cf32) * (size_t)n,
                                             cudaMemcpyDeviceToHost, c->stream)
                           : cudaSuccess;
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "batch output copy");
     return LPK_OK;
+}
+
+lpk_status lpk_batch_render(lpk_batch *b, lpk_unit_sink_fn sink, void *user) {
+    if (!b || !sink) return fail(b ? b->ctx : nullptr, LPK_EINVAL, "batch or sink is NULL");
+    lpk_ctx *c = b->ctx;
+    cudaSetDevice(c->device);
+    const int nu = (int)b->units.size();
+    // staging in the context's pinned pool (kept across batches and calls)
+    size_t bytes = 0;
+    for (int u = 0; u < nu; ++u) bytes += 2 * (((sizeof(lpk_cf32) * (size_t)b->units[u].round_len) + 255) / 256 * 256);
+    lpk_status pst = ensure_pinned(c, bytes);
+    if (pst) return pst;
+    {
+        char *h = (char *)c->h_pinned;
+        for (int p = 0; p < 2; ++p) {
+            b->staging[p].assign((size_t)nu, nullptr);
+            for (int u = 0; u < nu; ++u) {
+                b->staging[p][u] = (lpk_cf32 *)h;
+                h += ((sizeof(lpk_cf32) * (size_t)b->units[u].round_len) + 255) / 256 * 256;
+            }
+        }
+    }
+    std::vector<char> stopped((size_t)nu, 0);
+    auto deliver = [&](int64_t round, int p) -> lpk_status {
+        cudaError_t e = cudaEventSynchronize(b->copied[p]);
+        if (e != cudaSuccess) return cuda_fail(c, e, "output copy wait");
+        for (int u = 0; u < nu; ++u) {
+            int64_t i0, n;
+            unit_extent(b, round, u, i0, n);
+            if (n <= 0 || stopped[u]) continue;
+            int32_t flow = sink(user, u, b->staging[p][u], n);
+            if (flow < 0) return fail(c, LPK_EINVAL, "sink reported an error");
+            if (flow == 1) stopped[u] = 1;
+        }
+        return LPK_OK;
+    };
+    lpk_status st = LPK_OK;
+    for (int64_t r = 0; r < b->n_rounds && !st; ++r) {
+        if ((st = lpk_batch_run(b, r))) break;
+        const int p = b->last_parity;
+        // copies of round r on the copy stream, after the round's graph
+        cudaError_t e = cudaStreamWaitEvent(b->copy, b->done[p], 0);
+        for (int u = 0; u < nu && e == cudaSuccess; ++u) {
+            int64_t i0, n;
+            unit_extent(b, r, u, i0, n);
+            if (n > 0 && !stopped[u])
+                e = cudaMemcpyAsync(b->staging[p][u], b->h_units[u].out[p], sizeof(lpk_cf32) * (size_t)n,
+                                    cudaMemcpyDeviceToHost, b->copy);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(b->copied[p], b->copy);
+        if (e != cudaSuccess) { st = cuda_fail(c, e, "output copy"); break; }
+        if (r > 0) st = deliver(r - 1, p ^ 1);  // round r - 1 while round r renders
+    }
+    if (!st && b->n_rounds > 0) st = deliver(b->n_rounds - 1, b->last_parity);
+    cudaStreamSynchronize(b->copy);
+    return st;
 }
 
 lpk_status lpk_batch_set_config(lpk_batch *b, int32_t variant, int32_t blocks_per_sm) {

@@ -286,16 +286,24 @@ __device__ __forceinline__ float2 noise_pair(uint64_t seed, int64_t g) {
     return make_float2(__fmul_rn(rr, c), __fmul_rn(rr, s));
 }
 
-// One increment σ·z_k of the receiver clock's white-FM walk at master index
-// k: a counter-based normal (Philox block keyed by the clock seed), so any
+// Increments σ·z_k of the receiver clock's white-FM walk at master indices
+// k = 4q .. 4q+3: one Philox block (counter q, tag "CLOK", keyed by the
+// clock seed) gives two Box–Muller pairs in f32. Counter-based, so any
 // chunking or GPU regenerates the same walk.
-__device__ __forceinline__ double walk_increment(uint64_t seed, int64_t k, double sigma) {
-    uint4 x = philox4x32_10(make_uint4((uint32_t)(uint64_t)k, (uint32_t)((uint64_t)k >> 32), 0x434C4F4Bu, 0u),
-                            make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
-    float u1 = __fmul_rn(__fadd_rn((float)(x.x >> 8), 1.0f), 0x1.0p-24f);
-    float u2 = __fmul_rn((float)(x.y >> 8), 0x1.0p-24f);
-    float z = __fmul_rn(sqrtf(__fmul_rn(-2.0f, logf(u1))), cosf(__fmul_rn(6.28318548f, u2)));
-    return __dmul_rn(sigma, (double)z);
+__device__ __forceinline__ void walk_increments4(uint64_t seed, int64_t q, double sigma, double z[4]) {
+    const uint4 x = philox4x32_10(make_uint4((uint32_t)(uint64_t)q, (uint32_t)((uint64_t)q >> 32), 0x434C4F4Bu, 0u),
+                                  make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+    const uint32_t ua[2] = {x.x, x.z}, ub[2] = {x.y, x.w};
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+        const float u1 = __fmul_rn(__fadd_rn((float)(ua[p] >> 8), 1.0f), 0x1.0p-24f);
+        const float u2 = __fmul_rn((float)(ub[p] >> 8), 0x1.0p-24f);
+        const float r = sqrtf(__fmul_rn(-2.0f, logf(u1)));
+        float sn, cs;
+        sincosf(__fmul_rn(6.28318548f, u2), &sn, &cs);
+        z[2 * p] = __dmul_rn(sigma, (double)__fmul_rn(r, cs));
+        z[2 * p + 1] = __dmul_rn(sigma, (double)__fmul_rn(r, sn));
+    }
 }
 
 // AWGN then PostOp::apply in chain order (channel/mod.rs:323-334,

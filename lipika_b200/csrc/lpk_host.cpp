@@ -730,26 +730,16 @@ lpk_status lpk_generate_scene(lpk_scene *s, uint64_t seed_base, double round_s, 
         const int64_t rounds = lpk_batch_n_rounds(batch);
         if ((flags & LPK_GEN_AUTOTUNE) && rounds > 0 && (st = lpk_batch_autotune(batch, rounds / 2, 2, nullptr)))
             return st;
-        int64_t cap = 0;
-        for (size_t k = 0; k < units.size(); ++k) {
-            int64_t i0, n;
-            lpk_batch_round_extent(batch, 0, (int32_t)k, &i0, &n);
-            cap = std::max(cap, n);
-        }
-        std::vector<lpk_cf32> host((size_t)std::max<int64_t>(cap, 1));
-        std::vector<char> stopped(units.size(), 0);
-        for (int64_t rd = 0; rd < rounds; ++rd) {
-            if ((st = lpk_batch_run(batch, rd))) return st;
-            for (size_t k = 0; k < units.size(); ++k) {
-                int64_t i0, n;
-                lpk_batch_round_extent(batch, rd, (int32_t)k, &i0, &n);
-                if (n <= 0 || stopped[k]) continue;
-                if ((st = lpk_batch_copy_out(batch, (int32_t)k, host.data(), (int64_t)host.size()))) return st;
-                int32_t flow = sink(user, unit_work[k], host.data(), n);
-                if (flow < 0) return host_fail(LPK_EINVAL, "sink reported an error");
-                if (flow == 1) stopped[k] = 1;
-            }
-        }
+        struct Map {
+            lpk_unit_sink_fn sink;
+            void *user;
+            const int32_t *work;
+        } map{sink, user, unit_work.data()};
+        auto fwd = [](void *m, int32_t u, const lpk_cf32 *chunk, int64_t n) -> int32_t {
+            Map *mp = (Map *)m;
+            return mp->sink(mp->user, mp->work[u], chunk, n);
+        };
+        if ((st = lpk_batch_render(batch, fwd, &map))) return st;
     }
     for (int32_t w : rest) {
         const int32_t r = s->work[w].first, b = s->work[w].second;

@@ -12,13 +12,15 @@
 
 namespace lpk {
 
-// Cached carries of one receiver clock walk (seed, master rate, step σ).
+// Cached block totals and group sums of one receiver clock walk (seed,
+// master rate, step σ).
 struct WalkState {
     uint64_t seed = 0;
     double fm = 0.0, sigma = 0.0;
-    int64_t nb_done = 0;   // blocks whose totals and carries are known
-    int64_t cap = 0;
-    double *d_tot = nullptr, *d_carry = nullptr;
+    int64_t nb_done = 0;   // blocks whose totals are known
+    int64_t g_known = 0;   // groups whose sums are stored
+    int64_t cap = 0;       // blocks the arrays hold
+    double *d_tot = nullptr, *d_carry = nullptr, *d_gsum = nullptr;
 };
 }  // namespace lpk
 
@@ -77,8 +79,13 @@ inline bool use_split(const lpk_band_desc *d) {
     return d->solver == LPK_SOLVER_SPLIT && d->rx_kind == LPK_RX_STATIONARY && !d->has_antenna;
 }
 cudaError_t launch_or_flags(const uint32_t *d_uw, uint8_t *d_unocc, int32_t n_active, int mode, cudaStream_t s);
+// Totals of scan blocks [b_from, b_to).
 cudaError_t launch_walk_totals(uint64_t seed, double sigma, int64_t b_from, int64_t b_to, double *d_tot,
-                               double *d_carry, cudaStream_t s);
+                               cudaStream_t s);
+// carry(b) for b in [bA, bB] (totals below bB known; sums of groups below
+// g_known stored in d_gsum; afterwards those below bB / kGroupBlocks are).
+cudaError_t launch_walk_carries(const double *d_tot, double *d_gsum, int64_t g_known, int64_t bA, int64_t bB,
+                                double *d_carry, cudaStream_t s);
 cudaError_t launch_walk_materialize(uint64_t seed, double sigma, const double *d_carry, int64_t kA, int64_t kB,
                                     double *d_eps, cudaStream_t s);
 // Device walk for a band chunk: ensure carries, materialise ε over the
@@ -89,6 +96,9 @@ int64_t walk_span(const lpk_band_desc *d, int64_t i0, int64_t n, int64_t *kA);
 // Record a profiling event pair around a fan-out launch (no-op when off).
 void prof_begin(lpk_ctx *ctx);
 void prof_end(lpk_ctx *ctx);
+// Take the next profiling event pair for a fan-out that is timed by event
+// nodes inside a graph (false when profiling is off).
+bool prof_take(lpk_ctx *ctx, cudaEvent_t &a, cudaEvent_t &b);
 cudaError_t launch_fp64_probe(double *d_out, int blocks, int iters, cudaStream_t s);
 cudaError_t launch_solve(const DevTx *d_tx, int32_t tx, const double *d_obs, const double *d_t, int64_t n,
                          double epoch, int32_t iterations, double inv_c, double *d_temit, double *d_range,

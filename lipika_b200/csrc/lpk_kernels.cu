@@ -126,16 +126,13 @@ k_walk_block(uint64_t seed, double sigma, int64_t b0, double *__restrict__ total
     }
 }
 
-// carry(b + 1) = carry(b) + total(b), sequentially, for the new blocks.
-__global__ void k_walk_carry(const double *__restrict__ totals, double *__restrict__ carry, int64_t b_from,
-                             int64_t b_to) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    if (b_from == 0) carry[0] = 0.0;
-    double c = carry[b_from];
-    for (int64_t b = b_from; b < b_to; ++b) {
-        c = __dadd_rn(c, totals[b]);
-        carry[b + 1] = c;
-    }
+// carry(b) for b in [bA, bB], one block per carry group (lpk_walk.cuh).
+__global__ void __launch_bounds__(kGroupThreads)
+k_walk_carries(const double *__restrict__ tot, double *__restrict__ gsum, int64_t g_known, int64_t bA, int64_t bB,
+               double *__restrict__ carry) {
+    __shared__ double sh[65];
+    const int64_t g = bA / kGroupBlocks + blockIdx.x;
+    walk_group_carries(tot, gsum, g_known, bA, bB, g, blockIdx.x == 0, carry, sh);
 }
 
 __global__ void __launch_bounds__(kBlock) k_band_delta(const DevBand b, double *__restrict__ out) {
@@ -189,12 +186,17 @@ cudaError_t launch_or_flags(const uint32_t *d_uw, uint8_t *d_unocc, int32_t n_ac
 }
 
 cudaError_t launch_walk_totals(uint64_t seed, double sigma, int64_t b_from, int64_t b_to, double *d_tot,
-                               double *d_carry, cudaStream_t s) {
+                               cudaStream_t s) {
     if (b_to <= b_from) return cudaSuccess;
     k_walk_block<<<(unsigned)(b_to - b_from), kWalkThreads, 0, s>>>(seed, sigma, b_from, d_tot, nullptr, nullptr, 0, -1);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    k_walk_carry<<<1, 32, 0, s>>>(d_tot, d_carry, b_from, b_to);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_walk_carries(const double *d_tot, double *d_gsum, int64_t g_known, int64_t bA, int64_t bB,
+                                double *d_carry, cudaStream_t s) {
+    if (bB < bA) return cudaSuccess;
+    const int64_t groups = bB / kGroupBlocks - bA / kGroupBlocks + 1;
+    k_walk_carries<<<(unsigned)groups, kGroupThreads, 0, s>>>(d_tot, d_gsum, g_known, bA, bB, d_carry);
     return cudaGetLastError();
 }
 

@@ -6,7 +6,7 @@
 // or an embedding where only pre-registered buffers may be touched. For them,
 // lpk_band_chunk_device_static does what lpk_band_chunk_device does — the
 // active list, the per-transmitter occlusion words and the receiver clock
-// walk (block totals, carries, the materialised walk) — in one file-scope
+// walk (block totals, group sums, carries, the materialised walk) — in one file-scope
 // static device array instead of the context's growable scratch.
 //
 // The array lives on every GPU that loads the library until the process exits.
@@ -27,8 +27,9 @@ constexpr size_t kOffActive = 0;
 constexpr size_t kOffWords = kOffActive + sizeof(int32_t) * kMaxActive;
 constexpr size_t kOffTotals = kOffWords + sizeof(uint32_t) * kMaxActive;
 constexpr size_t kOffCarry = kOffTotals + sizeof(double) * kMaxWalkBlocks;
-constexpr size_t kOffEps = kOffCarry + sizeof(double) * (kMaxWalkBlocks + 1) + 248;  // keep 256-byte alignment
-constexpr size_t kStaticBytes = kOffEps + sizeof(double) * kMaxWalkSpan;           // 10.0 MiB
+constexpr size_t kOffGsum = kOffCarry + sizeof(double) * (kMaxWalkBlocks + 1);
+constexpr size_t kOffEps = (kOffGsum + sizeof(double) * (kMaxWalkBlocks / lpk::kGroupBlocks + 1) + 255) / 256 * 256;
+constexpr size_t kStaticBytes = kOffEps + sizeof(double) * kMaxWalkSpan;  // 10.0 MiB
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
 
@@ -85,15 +86,16 @@ extern "C" lpk_status lpk_band_chunk_device_static(lpk_ctx *c, const lpk_band_de
     int32_t *d_active = (int32_t *)(base + kOffActive);
     uint32_t *d_words = (uint32_t *)(base + kOffWords);
     double *d_tot = (double *)(base + kOffTotals), *d_carry = (double *)(base + kOffCarry);
+    double *d_gsum = (double *)(base + kOffGsum);
     double *d_eps = (double *)(base + kOffEps);
     cudaError_t e = cudaMemcpyAsync(d_active, active, sizeof(int32_t) * (size_t)n_active, cudaMemcpyHostToDevice,
                                     c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_words, 0, sizeof(uint32_t) * kMaxActive, c->stream);
     if (e == cudaSuccess && span) {
-        // The walk's carries are rebuilt from block 0 on every call: nothing
-        // of an earlier call is trusted.
-        e = cudaMemsetAsync(d_carry, 0, sizeof(double), c->stream);
-        if (e == cudaSuccess && need > 0) e = launch_walk_totals(band->clock_seed, sigma, 0, need, d_tot, d_carry, c->stream);
+        // The walk's totals and carries are rebuilt from block 0 on every
+        // call: nothing of an earlier call is trusted.
+        if (need > 0) e = launch_walk_totals(band->clock_seed, sigma, 0, need, d_tot, c->stream);
+        if (e == cudaSuccess) e = launch_walk_carries(d_tot, d_gsum, 0, kA / kWalkBlock, need, d_carry, c->stream);
         if (e == cudaSuccess) e = launch_walk_materialize(band->clock_seed, sigma, d_carry, kA, kA + span - 1, d_eps, c->stream);
         b.eps = d_eps;
         b.eps_k0 = kA;

@@ -137,6 +137,8 @@ SIGNATURES = {
     "lpk_batch_run": (C.c_int32, [_VP, C.c_int64]),
     "lpk_batch_output": (C.c_int32, [_VP, C.c_int32, C.POINTER(_VP)]),
     "lpk_batch_copy_out": (C.c_int32, [_VP, C.c_int32, _CF, C.c_int64]),
+    "lpk_batch_reset": (C.c_int32, [_VP]),
+    "lpk_batch_render": (C.c_int32, [_VP, UNIT_SINK_FN, _VP]),
     "lpk_batch_set_config": (C.c_int32, [_VP, C.c_int32, C.c_int32]),
     "lpk_batch_get_config": (C.c_int32, [_VP, _I32, _I32, _I32]),
     "lpk_batch_autotune": (C.c_int32, [_VP, C.c_int64, C.c_int32, _D]),
@@ -296,12 +298,23 @@ class Batch:
         return tab.reshape(nv, 2)
 
     def render(self):
-        """Every round; returns one complex64 array per unit."""
+        """Every round through lpk_batch_render (double-buffered copies to
+        pinned staging); returns one complex64 array per unit."""
         outs = [[] for _ in range(self.n_units)]
-        for r in range(self.n_rounds):
-            self.run(r)
-            for u in range(self.n_units):
-                n = self.extent(r, u)[1]
-                if n > 0:
-                    outs[u].append(self.output(u)[:n].copy())
+        err: list = []
+
+        def _sink(_user, u, ptr, n):
+            try:
+                arr = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_float)), shape=(2 * n,)).copy()
+                outs[u].append(arr.view(np.complex64))
+                return 0
+            except BaseException as e:
+                err.append(e)
+                return -1
+
+        cb = UNIT_SINK_FN(_sink)
+        code = lib().lpk_batch_render(self.h, cb, None)
+        if err:
+            raise err[0]
+        self.ctx.check(code)
         return [np.concatenate(o) if o else np.zeros(0, np.complex64) for o in outs]

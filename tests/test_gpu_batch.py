@@ -161,3 +161,23 @@ def test_generate_scene_matches_generate_band(ctx):
         assert x.shape == y.shape
         assert _rel(x, y) <= SPLIT_RTOL, (w, _rel(x, y))
     prep.close()
+
+
+def test_batch_profiling_times_each_fanout_without_changing_bits(ctx):
+    prep = P.Prepared(_uneven_scene(), ctx)
+    units = _units(prep, N.LPK_SOLVER_SPLIT)
+    L = N.lib()
+    b = N.Batch(ctx, units, round_s=0.25)
+    ctx.check(L.lpk_profile_reset(ctx.h))
+    ctx.check(L.lpk_profile_enable(ctx.h, 1))
+    got = b.render()
+    ms, fan, alln = C.c_double(), C.c_int64(), C.c_int64()
+    ctx.check(L.lpk_profile_read(ctx.h, C.byref(ms), C.byref(fan), C.byref(alln)))
+    ctx.check(L.lpk_profile_enable(ctx.h, 0))
+    assert fan.value == b.n_rounds  # one timed persistent fan-out per round
+    assert alln.value == 4 * b.n_rounds  # walk scan, carries, anchors, fan-out
+    assert ms.value > 0.0
+    ref = N.Batch(ctx, units, round_s=0.25).render()
+    for x, y in zip(got, ref):
+        assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+    prep.close()
