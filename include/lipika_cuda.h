@@ -306,6 +306,62 @@ lpk_status lpk_batch_get_config(const lpk_batch *b, int32_t *variant, int32_t *b
 lpk_status lpk_batch_autotune(lpk_batch *b, int64_t round, int32_t reps, double *ms_table);
 
 /* ------------------------------------------------------------------ */
+/* Converged emission solve and its learned warm start                 */
+/* ------------------------------------------------------------------ */
+/* The reference stops after two fixed-point iterations from t - 70 ms
+ * (src/channel/mod.rs:49-101, NEWTON_ITERATIONS = 2), which is what the
+ * fan-out reproduces. lpk_solve_converged instead iterates to a tolerance
+ * (the delay truth the reference's own tests compare against,
+ * src/channel/mod.rs:355-383, runs four iterations), on the same
+ * trajectory model (lerp table, linearised Sagnac), from one of three
+ * starts: the reference's t - 70 ms (LAG), the range at the reception time
+ * R(t)/c (GEOMETRIC), or R(t)/c plus the light-time correction predicted by
+ * a trained lpk_mlp (LEARNED). A start that does not converge within
+ * max_iter falls back to LAG; iters[i] counts every map evaluation (-1 if
+ * even the fallback did not converge) and start_err[i] (may be NULL) is
+ * |start - converged delay| in seconds. No reference counterpart. */
+enum { LPK_START_LAG = 0, LPK_START_GEOMETRIC = 1, LPK_START_LEARNED = 2 };
+enum { LPK_ITER_FIXED_POINT = 0, LPK_ITER_NEWTON = 1 };
+#define LPK_MLP_N_FEATURES 8
+#define LPK_MLP_N_PARAMS 4801  /* W1 64x8, b1 64, W2 64x64, b2 64, w3 64, b3 (FP32, row-major) */
+#define LPK_MLP_N_NORM 18      /* feature means (8), feature stds (8), target mean, target std (µs) */
+typedef struct lpk_mlp lpk_mlp;
+
+lpk_status lpk_solve_converged(lpk_ctx *ctx, int32_t tx, const double *rx_ecef, double epoch,
+                               const double *t_rel_utc, int64_t n, double tol_s, int32_t max_iter,
+                               int32_t scheme, int32_t start, const lpk_mlp *mlp, double *t_emit,
+                               int32_t *iters, float *start_err);
+/* The network's raw input features at the reception times: line-of-sight
+ * unit vector (3), R/c, range rate / c, v_x / c, v_y / c, Sagnac rate of
+ * the line of sight (n x 8, host memory). */
+lpk_status lpk_solve_features(lpk_ctx *ctx, int32_t tx, const double *rx_ecef, double epoch,
+                              const double *t_rel_utc, int64_t n, float *features);
+/* A tanh MLP 8 -> 64 -> 64 -> 1 whose output, de-normalised, is the
+ * light-time correction tau - R/c in microseconds. Glorot-uniform initial
+ * weights from `seed`. Forward, backward and the weight gradients run on
+ * the tensor cores (BF16 operands, FP32 accumulation); Adam updates FP32
+ * master weights. */
+lpk_status lpk_mlp_create(lpk_ctx *ctx, uint64_t seed, lpk_mlp **out);
+void lpk_mlp_destroy(lpk_mlp *mlp);
+lpk_status lpk_mlp_get_params(const lpk_mlp *mlp, float *params, float *norm);
+lpk_status lpk_mlp_set_params(lpk_mlp *mlp, const float *params, const float *norm);
+/* y = MLP(x) on n rows of normalised features (host memory). */
+lpk_status lpk_mlp_forward(lpk_mlp *mlp, const float *x, int64_t n, float *y);
+/* Mean squared error over n rows and its gradient (LPK_MLP_N_PARAMS floats,
+ * the parameter layout above); host memory. */
+lpk_status lpk_mlp_loss_grad(lpk_mlp *mlp, const float *x, const float *t, int64_t n, double *loss,
+                             float *grad);
+/* Train on n_train reception times uniform in [t0, t1) of transmitter tx
+ * seen from rx_ecef: the converged Newton solver (geometric start) produces
+ * the targets on the GPU, the normalisation comes from the training set,
+ * then `steps` Adam steps on batches of `batch` rows with a cosine-decayed
+ * learning rate. loss_curve (may be NULL) receives each step's batch MSE in
+ * normalised units. */
+lpk_status lpk_mlp_fit(lpk_mlp *mlp, int32_t tx, const double *rx_ecef, double epoch, double t0, double t1,
+                       int64_t n_train, int32_t steps, int32_t batch, float lr, uint64_t seed,
+                       float *loss_curve);
+
+/* ------------------------------------------------------------------ */
 /* Host-level mirror of src/pipeline.rs (scene -> per-band streams)     */
 /* ------------------------------------------------------------------ */
 typedef struct lpk_scene lpk_scene;

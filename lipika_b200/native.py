@@ -29,6 +29,9 @@ LPK_RX_STATIONARY, LPK_RX_PER_SAMPLE = 0, 1
 LPK_POST_GAIN, LPK_POST_NONLINEARITY, LPK_POST_ADC = 0, 1, 2
 LPK_SOLVER_REFERENCE, LPK_SOLVER_SPLIT = 0, 1
 LPK_NOISE_OFF, LPK_NOISE_ON, LPK_GEN_DEVICE_CLOCK, LPK_GEN_SPLIT, LPK_GEN_AUTOTUNE = 0, 1, 2, 4, 8
+LPK_START_LAG, LPK_START_GEOMETRIC, LPK_START_LEARNED = 0, 1, 2
+LPK_ITER_FIXED_POINT, LPK_ITER_NEWTON = 0, 1
+MLP_N_FEATURES, MLP_N_PARAMS, MLP_N_NORM = 8, 4801, 18
 
 
 class LpkError(RuntimeError):
@@ -100,6 +103,7 @@ _D = C.POINTER(C.c_double)
 _I32 = C.POINTER(C.c_int32)
 _U8 = C.POINTER(C.c_uint8)
 _CF = C.POINTER(CF32)
+_F = C.POINTER(C.c_float)
 _VP = C.c_void_p
 
 # name -> (restype, argtypes); every entry point of include/lipika_cuda.h
@@ -155,6 +159,17 @@ SIGNATURES = {
     "lpk_generate_band_to_file": (C.c_int32, [_VP, C.c_int32, C.c_int32, C.c_uint64, C.c_int32, C.c_int64,
                                               C.c_int32, C.c_char_p, C.POINTER(BandResult)]),
     "lpk_generate_scene": (C.c_int32, [_VP, C.c_uint64, C.c_double, C.c_int32, UNIT_SINK_FN, _VP]),
+    "lpk_solve_converged": (C.c_int32, [_VP, C.c_int32, _D, C.c_double, _D, C.c_int64, C.c_double, C.c_int32,
+                                        C.c_int32, C.c_int32, _VP, _D, _I32, _F]),
+    "lpk_solve_features": (C.c_int32, [_VP, C.c_int32, _D, C.c_double, _D, C.c_int64, _F]),
+    "lpk_mlp_create": (C.c_int32, [_VP, C.c_uint64, C.POINTER(_VP)]),
+    "lpk_mlp_destroy": (None, [_VP]),
+    "lpk_mlp_get_params": (C.c_int32, [_VP, _F, _F]),
+    "lpk_mlp_set_params": (C.c_int32, [_VP, _F, _F]),
+    "lpk_mlp_forward": (C.c_int32, [_VP, _F, C.c_int64, _F]),
+    "lpk_mlp_loss_grad": (C.c_int32, [_VP, _F, _F, C.c_int64, _D, _F]),
+    "lpk_mlp_fit": (C.c_int32, [_VP, C.c_int32, _D, C.c_double, C.c_double, C.c_double, C.c_int64, C.c_int32,
+                                C.c_int32, C.c_float, C.c_uint64, _F]),
     "lpk_clock_new": (C.c_int32, [C.POINTER(A.ClockCfg), C.c_double, C.c_double, C.c_uint64, C.POINTER(_VP)]),
     "lpk_clock_delta_t": (C.c_int32, [_VP, _D, C.c_int64, _D]),
     "lpk_clock_free": (None, [_VP]),
@@ -318,3 +333,83 @@ class Batch:
             raise err[0]
         self.ctx.check(code)
         return [np.concatenate(o) if o else np.zeros(0, np.complex64) for o in outs]
+
+
+def _fp(a):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_F)
+
+
+class Mlp:
+    """lpk_mlp: the warm-start network of the converged emission solve."""
+
+    def __init__(self, ctx: Context, seed: int = 0):
+        self.ctx = ctx
+        h = _VP()
+        ctx.check(lib().lpk_mlp_create(ctx.h, seed & 0xFFFFFFFFFFFFFFFF, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            try:
+                lib().lpk_mlp_destroy(self.h)
+            except Exception:
+                pass
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def params(self):
+        p = np.zeros(MLP_N_PARAMS, np.float32)
+        nrm = np.zeros(MLP_N_NORM, np.float32)
+        self.ctx.check(lib().lpk_mlp_get_params(self.h, _fp(p), _fp(nrm)))
+        return p, nrm
+
+    def set_params(self, p, norm=None):
+        p = np.ascontiguousarray(p, np.float32)
+        nrm = None if norm is None else np.ascontiguousarray(norm, np.float32)
+        self.ctx.check(lib().lpk_mlp_set_params(self.h, _fp(p), None if nrm is None else _fp(nrm)))
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.zeros(len(x), np.float32)
+        self.ctx.check(lib().lpk_mlp_forward(self.h, _fp(x), len(x), _fp(y)))
+        return y
+
+    def loss_grad(self, x, t):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        g = np.zeros(MLP_N_PARAMS, np.float32)
+        loss = C.c_double()
+        self.ctx.check(lib().lpk_mlp_loss_grad(self.h, _fp(x), _fp(t), len(x), C.byref(loss), _fp(g)))
+        return loss.value, g
+
+    def fit(self, tx, rx_ecef, epoch, t0, t1, n_train=1 << 18, steps=1500, batch=4096, lr=3e-3, seed=1):
+        rx = np.ascontiguousarray(rx_ecef, np.float64)
+        curve = np.zeros(steps, np.float32)
+        self.ctx.check(lib().lpk_mlp_fit(self.h, tx, dptr(rx), epoch, t0, t1, n_train, steps, batch, lr,
+                                         seed & 0xFFFFFFFFFFFFFFFF, _fp(curve)))
+        return curve
+
+
+def solve_converged(ctx: Context, tx, rx_ecef, epoch, t_rel_utc, tol=1e-13, max_iter=12,
+                    scheme=LPK_ITER_NEWTON, start=LPK_START_LAG, mlp: "Mlp | None" = None):
+    """Converged emission solve: (t_emit, iterations, |start - converged| in s)."""
+    t = np.ascontiguousarray(t_rel_utc, np.float64)
+    rx = np.ascontiguousarray(rx_ecef, np.float64)
+    te = np.zeros(len(t))
+    it = np.zeros(len(t), np.int32)
+    err = np.zeros(len(t), np.float32)
+    ctx.check(lib().lpk_solve_converged(ctx.h, tx, dptr(rx), epoch, dptr(t), len(t), tol, max_iter, scheme, start,
+                                        mlp.h if mlp is not None else None, dptr(te),
+                                        it.ctypes.data_as(_I32), _fp(err)))
+    return te, it, err
+
+
+def solve_features(ctx: Context, tx, rx_ecef, epoch, t_rel_utc):
+    t = np.ascontiguousarray(t_rel_utc, np.float64)
+    rx = np.ascontiguousarray(rx_ecef, np.float64)
+    f = np.zeros((len(t), MLP_N_FEATURES), np.float32)
+    ctx.check(lib().lpk_solve_features(ctx.h, tx, dptr(rx), epoch, dptr(t), len(t), _fp(f)))
+    return f
