@@ -65,6 +65,8 @@ def _args():
                         "band: one launch pair per band chunk")
     p.add_argument("--round-s", type=float, default=8.0, help="seconds of scene time per batch round")
     p.add_argument("--no-autotune", action="store_true", help="keep the default split launch shape")
+    p.add_argument("--variant", type=int, default=-1,
+                   help="split launch shape (lpk_split_variant_info) instead of autotuning")
     return p.parse_args()
 
 
@@ -277,7 +279,10 @@ def run_ours(a):
     batch, tune = None, None
     if a.path == "batch":
         batch = N.Batch(ctx, [(d, act, n) for (d, act, n) in bands], a.round_s)
-        if not a.no_autotune and a.solver == "split":
+        if a.variant >= 0:
+            batch.set_config(a.variant)
+            ctx.check(L.lpk_ctx_set_split_variant(ctx.h, a.variant))
+        elif not a.no_autotune and a.solver == "split":
             tab = batch.autotune(rnd=batch.n_rounds // 2, reps=2)
             v, bps, mx = batch.config()
             tune = {"variant": v, "shape": dict(zip(("tile", "threads", "min_blocks"), N.split_variants()[v])),

@@ -87,6 +87,7 @@ __device__ __forceinline__ int find_slot_recs(const RoundDesc &rd, int64_t g) {
 __global__ void __launch_bounds__(kWalkThreads)
 k_batch_walk(const DevWalk *__restrict__ walks, const RoundDesc *__restrict__ rd) {
     __shared__ double warp_tot[kWalkThreads / 32];
+    __shared__ double stage[kWalkStageDoubles];
     const int64_t total = rd->total_walk_blocks;
     for (int64_t g = blockIdx.x; g < total; g += gridDim.x) {
         int w = 0;
@@ -97,10 +98,13 @@ k_batch_walk(const DevWalk *__restrict__ walks, const RoundDesc *__restrict__ rd
         double v[kWalkPer], offset;
         walk_block_prefix(dw.seed, dw.sigma, b, warp_tot, v, offset);
         if (threadIdx.x == kWalkThreads - 1) dw.totals[b] = __dadd_rn(offset, v[kWalkPer - 1]);
-        if (b >= rw.bA) {
-            const int64_t base = b * kWalkBlock + (int64_t)threadIdx.x * kWalkPer - rw.bA * kWalkBlock;
+        if (b >= rw.bA) {  // block-uniform
 #pragma unroll
-            for (int i = 0; i < kWalkPer; ++i) dw.partial[base + i] = __dadd_rn(offset, v[i]);
+            for (int i = 0; i < kWalkPer; ++i) stage[threadIdx.x * kWalkStageLd + i] = __dadd_rn(offset, v[i]);
+            __syncthreads();
+            double *dst = dw.partial + (b - rw.bA) * kWalkBlock;
+            for (int kk = threadIdx.x; kk < (int)kWalkBlock; kk += kWalkThreads) dst[kk] = stage[walk_stage_at(kk)];
+            __syncthreads();  // stage is rewritten by the next block
         }
     }
 }

@@ -272,18 +272,26 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
     return c;
 }
 
-// AWGN pair for (seed, global band-sample index): counter-based, so chunking
-// cannot change it. Box–Muller in f32.
-__device__ __forceinline__ float2 noise_pair(uint64_t seed, int64_t g) {
-    uint4 x = philox4x32_10(make_uint4((uint32_t)(uint64_t)g, (uint32_t)((uint64_t)g >> 32), 0x4E4F4953u, 0u),
-                            make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
-    float u1 = __fmul_rn(__fadd_rn((float)(x.x >> 8), 1.0f), 0x1.0p-24f);
-    float u2 = __fmul_rn((float)(x.y >> 8), 0x1.0p-24f);
+// AWGN for (seed, global band-sample index): one Philox block per pair of
+// indices 2p, 2p+1 (words 0-1 for 2p, words 2-3 for 2p+1), Box–Muller in
+// f32. Counter-based, so chunking cannot change it.
+__device__ __forceinline__ float2 box_muller(uint32_t a, uint32_t b) {
+    float u1 = __fmul_rn(__fadd_rn((float)(a >> 8), 1.0f), 0x1.0p-24f);
+    float u2 = __fmul_rn((float)(b >> 8), 0x1.0p-24f);
     float rr = sqrtf(__fmul_rn(-2.0f, logf(u1)));
     float ang = __fmul_rn(6.28318548f, u2);
     float s, c;
     sincosf(ang, &s, &c);
     return make_float2(__fmul_rn(rr, c), __fmul_rn(rr, s));
+}
+__device__ __forceinline__ uint4 noise_block(uint64_t seed, int64_t g) {
+    const uint64_t p = (uint64_t)g >> 1;
+    return philox4x32_10(make_uint4((uint32_t)p, (uint32_t)(p >> 32), 0x4E4F4953u, 0u),
+                         make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
+}
+__device__ __forceinline__ float2 noise_pair(uint64_t seed, int64_t g) {
+    const uint4 x = noise_block(seed, g);
+    return (g & 1) ? box_muller(x.z, x.w) : box_muller(x.x, x.y);
 }
 
 // Increments σ·z_k of the receiver clock's white-FM walk at master indices
@@ -306,14 +314,36 @@ __device__ __forceinline__ void walk_increments4(uint64_t seed, int64_t q, doubl
     }
 }
 
-// AWGN then PostOp::apply in chain order (channel/mod.rs:323-334,
-// rx/mod.rs:83-101), on one band sample.
+// PostOp::apply in chain order (rx/mod.rs:83-101), on one band sample.
+__device__ __forceinline__ float2 band_post(const DevBand &b, float re, float im);
+
+// AWGN then the receiver chain (channel/mod.rs:323-334, rx/mod.rs:83-101),
+// on one band sample.
 __device__ __forceinline__ float2 band_epilogue(const DevBand &b, float re, float im, int64_t g) {
     if (b.has_noise) {
         float2 z = noise_pair(b.noise_seed, g);
         re = __fadd_rn(re, __fmul_rn(b.noise_std, z.x));
         im = __fadd_rn(im, __fmul_rn(b.noise_std, z.y));
     }
+    return band_post(b, re, im);
+}
+
+// The same on the band-sample pair (g, g+1), g even: one Philox block.
+__device__ __forceinline__ void band_epilogue2(const DevBand &b, float re0, float im0, float re1, float im1,
+                                               int64_t g, float2 &o0, float2 &o1) {
+    if (b.has_noise) {
+        const uint4 x = noise_block(b.noise_seed, g);
+        const float2 z0 = box_muller(x.x, x.y), z1 = box_muller(x.z, x.w);
+        re0 = __fadd_rn(re0, __fmul_rn(b.noise_std, z0.x));
+        im0 = __fadd_rn(im0, __fmul_rn(b.noise_std, z0.y));
+        re1 = __fadd_rn(re1, __fmul_rn(b.noise_std, z1.x));
+        im1 = __fadd_rn(im1, __fmul_rn(b.noise_std, z1.y));
+    }
+    o0 = band_post(b, re0, im0);
+    o1 = band_post(b, re1, im1);
+}
+
+__device__ __forceinline__ float2 band_post(const DevBand &b, float re, float im) {
     for (int k = 0; k < b.n_post; ++k) {
         if (b.post_kind[k] == 0) {
             re = __fmul_rn(re, b.post_a[k]);

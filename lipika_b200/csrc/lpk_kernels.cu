@@ -110,6 +110,7 @@ __global__ void __launch_bounds__(kWalkThreads)
 k_walk_block(uint64_t seed, double sigma, int64_t b0, double *__restrict__ totals,
              const double *__restrict__ carry, double *__restrict__ eps, int64_t kA, int64_t kB) {
     __shared__ double warp_tot[kWalkThreads / 32];
+    __shared__ double stage[kWalkStageDoubles];
     const int64_t b = b0 + blockIdx.x;
     double v[kWalkPer], offset;
     walk_block_prefix(seed, sigma, b, warp_tot, v, offset);
@@ -118,11 +119,13 @@ k_walk_block(uint64_t seed, double sigma, int64_t b0, double *__restrict__ total
         return;
     }
     const double c = carry[b];
-    const int64_t base = b * kWalkBlock + (int64_t)threadIdx.x * kWalkPer;
 #pragma unroll
-    for (int i = 0; i < kWalkPer; ++i) {
-        int64_t k = base + i;
-        if (k >= kA && k <= kB) eps[k - kA] = __dadd_rn(c, __dadd_rn(offset, v[i]));
+    for (int i = 0; i < kWalkPer; ++i)
+        stage[threadIdx.x * kWalkStageLd + i] = __dadd_rn(c, __dadd_rn(offset, v[i]));
+    __syncthreads();
+    for (int kk = threadIdx.x; kk < (int)kWalkBlock; kk += kWalkThreads) {
+        const int64_t k = b * kWalkBlock + kk;
+        if (k >= kA && k <= kB) eps[k - kA] = stage[walk_stage_at(kk)];
     }
 }
 

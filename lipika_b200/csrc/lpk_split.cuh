@@ -50,7 +50,9 @@ constexpr double kSplitMargin = 1e-5;  // s
 // boundary falls inside the tile (otherwise nav_pm holds the tile's sign);
 // kRecGateOff: the transmitter is silent over the whole tile (gate off, or
 // an empty frame), so it adds nothing.
-enum : int32_t { kRecExact = 1, kRecNavVary = 2, kRecGateOff = 4 };
+// kRecCaWide: the C/A code phase of the tile spans too many chips for the
+// tile-relative chip index (the general modulo path is taken).
+enum : int32_t { kRecExact = 1, kRecNavVary = 2, kRecGateOff = 4, kRecCaWide = 8 };
 
 struct __align__(16) AnchorRec {
     double tu0, tu_hi;                // fit range; Δ origin tu0
@@ -66,6 +68,8 @@ struct __align__(16) AnchorRec {
     int32_t flags;
     int32_t nav_pm;                   // nav sign of the tile (1 with nav off; unused with kRecNavVary)
     int64_t sym_raw0, sym_pos0;       // framed kinds: raw symbol count at the tile start and its frame slot
+    double chip_fl0;                  // C/A: a whole chip count at or below the tile's first chip
+    int32_t chip_m0, pad;             // C/A: chip_fl0 mod 1023
 };
 
 // Lerp position at epoch-relative time t with the segment forced to `lo`
@@ -175,6 +179,8 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
     for (int i = 0; i < 3; ++i) r.p0a[i] = r.p0b[i] = r.p1a[i] = r.p1b[i] = 0.0;
     int64_t lo0s = 0, lo0e = 0, lo1s = 0, lo1e = 0;
     bool exact = exact_only;
+    r.chip_fl0 = 0.0;
+    r.chip_m0 = r.pad = 0;
     if (exact) {
         r.amp0 = r.amp1 = 0.0f;
         r.guard = r.ulp_q = r.tie = 0.0;
@@ -253,6 +259,16 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
             if (tx.has_repeat && !((te_e - te_s) * tx.rate + 3.0 < (double)tx.n_sym)) exact = true;
         }
     }
+    if (!exact && tx.sig_kind == kCa) {  // tile-relative chip index: chip_m0 + (floor(cp) - chip_fl0)
+        const double cs = (te_s - tx.epoch_rel) * kCaChipRate, ce = (te_e - tx.epoch_rel) * kCaChipRate;
+        const double f0 = floor(cs) - 2.0;
+        if (!(fabs(f0) < 1.0e15) || !(ce - f0 + 2.0 < 1023.0)) {
+            r.flags |= kRecCaWide;
+        } else {
+            r.chip_fl0 = f0;
+            r.chip_m0 = (int32_t)i64_rem_euclid((int64_t)f0, 1023);
+        }
+    }
     if (!exact && tx.sig_kind == kCa && tx.nav_kind != kNavOff) {
         double ns = (te_s - tx.epoch_rel) * kNavBitRate, ne = (te_e - tx.epoch_rel) * kNavBitRate;
         double fs_ = floor(ns), fe_ = floor(ne), g = r.guard * kNavBitRate;
@@ -284,6 +300,15 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
     if (exact) r.flags = kRecExact;
 }
 
+// Chunk index of sample s of this thread in a tile starting at chunk index
+// `first`: each thread holds pairs of adjacent samples (2·tid, 2·tid+1) in
+// every 2·THREADS-sample stride, so a pair shares one AWGN Philox block and
+// one 16-byte store.
+template <int THREADS>
+__device__ __forceinline__ int64_t tile_sample(int64_t first, int s) {
+    return first + (int64_t)(s >> 1) * (2 * THREADS) + 2 * (int64_t)threadIdx.x + (s & 1);
+}
+
 // Per-sample values shared by every transmitter of the band: local
 // reception time, clock offset, and the rounding offset of the first
 // trajectory query epoch + (tu - 70 ms), the same for every transmitter.
@@ -297,7 +322,7 @@ enum PassKind : int { kPassCa = 0, kPassCaNav, kPassBpsk, kPassOok, kPassQam, kP
 
 __device__ __forceinline__ int pass_kind(const DevTx &tx, const AnchorRec &r) {
     switch (tx.sig_kind) {
-    case kCa: return (r.flags & kRecNavVary) ? kPassCaNav : kPassCa;
+    case kCa: return (r.flags & (kRecNavVary | kRecCaWide)) ? kPassCaNav : kPassCa;
     case kBpsk: return kPassBpsk;
     case kOok: return kPassOok;
     case kQam16: return kPassQam;
@@ -315,7 +340,7 @@ __device__ __forceinline__ void split_baseband(const DevTx &tx, const AnchorRec 
         const double dt = __dsub_rn(te, tx.epoch_rel);
         const double cp = __dmul_rn(dt, kCaChipRate);
         const double fl = floor(cp), fr = cp - fl, g = guard * kCaChipRate;
-        ok &= fr >= g && fr <= 1.0 - g && fabs(fl) <= 1.0e9;
+        ok &= fr >= g && fr <= 1.0 - g;
         int nav = R.nav_pm;
         if constexpr (K == kPassCaNav) {
             const double nb = __dmul_rn(dt, kNavBitRate), nfl = floor(nb), nfr = nb - nfl, g2 = guard * kNavBitRate;
@@ -324,8 +349,16 @@ __device__ __forceinline__ void split_baseband(const DevTx &tx, const AnchorRec 
             if (tx.nav_kind == kNavDummy) nav = nav_bit_pm(tx.nav_seed, bi);
             else nav = tx.nav_n == 0 ? 1 : tx.nav_bits[bi < 0 ? 0 : (bi < tx.nav_n ? bi : tx.nav_n - 1)];
         }
-        int m = (int)fmax(fmin(fl, 1.0e9), -1.0e9) % 1023;
-        m += m < 0 ? 1023 : 0;
+        int m;
+        if constexpr (K == kPassCa) {  // within [0, 2045) for every sample in the fit range
+            m = R.chip_m0 + (int)(fl - R.chip_fl0);
+            m -= m >= 1023 ? 1023 : 0;
+            m = (unsigned)m < 1023u ? m : 0;  // samples outside the fit range are redone exactly
+        } else {
+            ok &= fabs(fl) <= 1.0e9;
+            m = (int)fmax(fmin(fl, 1.0e9), -1.0e9) % 1023;
+            m += m < 0 ? 1023 : 0;
+        }
         const int chip = ((tx.chip_neg[m >> 5] >> (m & 31)) & 1u) ? -nav : nav;
         bre = (float)chip;
     } else if constexpr (K == kPassBpsk || K == kPassOok || K == kPassQam) {  // frame_index, signal/mod.rs:109-115
@@ -419,7 +452,7 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
         redo |= (unsigned)!ok << s;
         if constexpr (DBG) {
             if ((fit >> s) & 1u) {
-                const int64_t j = first + s * THREADS + threadIdx.x;
+                const int64_t j = tile_sample<THREADS>(first, s);
                 dbg_phase[j] = rr;
                 dbg_temit[j] = te;
                 dbg_delay[j] = delay;
@@ -440,23 +473,27 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
     float ar[S], ai[S];
     unsigned live = 0, fit = 0;
     const double tu0 = n_active > 0 ? srec[0].tu0 : 0.0, tu_hi = n_active > 0 ? srec[0].tu_hi : 0.0;
+    static_assert(S % 2 == 0, "samples are held in adjacent pairs");
 #pragma unroll
     for (int s = 0; s < S; ++s) {
-        const int64_t j = first + s * THREADS + threadIdx.x;
+        // A sample outside the chunk takes the values of the nearest chunk
+        // sample (in the same tile), so every lane computes on valid inputs;
+        // its `live` bit stays clear and nothing of it is stored.
+        const int64_t j = tile_sample<THREADS>(first, s);
         const bool lv = j >= 0 && j < b.n;
+        const int64_t jc = j < 0 ? 0 : (j >= b.n ? b.n - 1 : j);
         ar[s] = ai[s] = 0.0f;
-        sc[s] = SampleCtx{0.0, 0.0, 0.0};
-        if (lv) {
-            const double tl = __ddiv_rn((double)(b.i0 + j), b.fs);  // src/pipeline.rs:918
-            const double dl = band_delta(b, j, tl);
-            const double tu = __dsub_rn(tl, dl);                     // :927
-            const double t0q = __dsub_rn(tu, kEmissionLag);
-            const double s0 = __dadd_rn(b.epoch, t0q);
-            sc[s] = SampleCtx{tl, dl, __dsub_rn(__dsub_rn(s0, b.epoch), t0q)};
-            live |= 1u << s;
-            // the fit range depends only on the tile: the same for every transmitter
-            fit |= (unsigned)(tu >= tu0 && tu <= tu_hi) << s;
-        }
+        const double tl = __ddiv_rn((double)(b.i0 + jc), b.fs);  // src/pipeline.rs:918
+        const double dl = band_delta(b, jc, tl);
+        const double tu = __dsub_rn(tl, dl);                      // :927
+        const double t0q = __dsub_rn(tu, kEmissionLag);
+        const double s0 = __dadd_rn(b.epoch, t0q);
+        sc[s] = SampleCtx{tl, dl, __dsub_rn(__dsub_rn(s0, b.epoch), t0q)};
+        live |= (unsigned)lv << s;
+        // the fit range depends only on the tile: the same for every
+        // transmitter (the pass sees `fit & live`: a sample outside the
+        // chunk is never stored, not even as a diagnostic)
+        fit |= (unsigned)(tu >= tu0 && tu <= tu_hi) << s;
     }
     for (int k = 0; k < n_active; ++k) {
         const AnchorRec &R = srec[k];
@@ -470,10 +507,10 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
 #define LPK_PASS(KIND)                                                                                           \
     do {                                                                                                         \
         if (kink)                                                                                                \
-            split_pass<KIND, DBG, true, S, THREADS>(T, R, b.epoch, sc, fit, ar, ai, redo, first, dbg_phase,      \
+            split_pass<KIND, DBG, true, S, THREADS>(T, R, b.epoch, sc, fit & live, ar, ai, redo, first, dbg_phase,      \
                                                     dbg_temit, dbg_delay);                                       \
         else                                                                                                     \
-            split_pass<KIND, DBG, false, S, THREADS>(T, R, b.epoch, sc, fit, ar, ai, redo, first, dbg_phase,     \
+            split_pass<KIND, DBG, false, S, THREADS>(T, R, b.epoch, sc, fit & live, ar, ai, redo, first, dbg_phase,     \
                                                      dbg_temit, dbg_delay);                                      \
     } while (0)
             switch (pass_kind(T, R)) {
@@ -500,7 +537,7 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
                 ai[s] = __fadd_rn(ai[s], ci);
             }
             if constexpr (DBG) {
-                const int64_t j = first + s * THREADS + threadIdx.x;
+                const int64_t j = tile_sample<THREADS>(first, s);
                 dbg_phase[j] = ph;
                 dbg_temit[j] = te;
                 dbg_delay[j] = rg * b.inv_c;
@@ -508,9 +545,22 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
         }
     }
 #pragma unroll
-    for (int s = 0; s < S; ++s) {
-        const int64_t j = first + s * THREADS + threadIdx.x;
-        if ((live >> s) & 1u) out[j] = band_epilogue(b, ar[s], ai[s], b.i0 + j);
+    for (int s = 0; s < S; s += 2) {  // g = b.i0 + j is even: the pair shares one noise block
+        const int64_t j = tile_sample<THREADS>(first, s);
+        const unsigned lv = (live >> s) & 3u;
+        if (lv == 3u) {
+            float2 o0, o1;
+            band_epilogue2(b, ar[s], ai[s], ar[s + 1], ai[s + 1], b.i0 + j, o0, o1);
+            if ((j & 1) == 0) {
+                *reinterpret_cast<float4 *>(out + j) = make_float4(o0.x, o0.y, o1.x, o1.y);
+            } else {
+                out[j] = o0;
+                out[j + 1] = o1;
+            }
+        } else {
+            if (lv & 1u) out[j] = band_epilogue(b, ar[s], ai[s], b.i0 + j);
+            if (lv & 2u) out[j + 1] = band_epilogue(b, ar[s + 1], ai[s + 1], b.i0 + j + 1);
+        }
     }
 }
 

@@ -57,6 +57,14 @@ __device__ __forceinline__ void walk_block_prefix(uint64_t seed, double sigma, i
     __syncthreads();  // warp_tot may be reused by the caller's next block
 }
 
+// Shared staging of one scan block's 4096 values, so that global stores
+// run coalesced: thread t's run of kWalkPer values sits at row t (rows
+// padded by one double against bank conflicts); element k of the block is
+// walk_stage_at(k).
+constexpr int kWalkStageLd = kWalkPer + 1;
+constexpr int kWalkStageDoubles = kWalkThreads * kWalkStageLd;
+__device__ __forceinline__ int walk_stage_at(int k) { return (k / kWalkPer) * kWalkStageLd + k % kWalkPer; }
+
 // Inclusive warp scan in a fixed order (Hillis–Steele): lane l's result
 // depends only on lanes 0..l.
 __device__ __forceinline__ double warp_incl_scan(double v, int lane) {

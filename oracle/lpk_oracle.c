@@ -143,15 +143,18 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
     out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
 }
 
-/* The CUDA backend's AWGN spec: one Philox block per (noise seed, global
- * band-sample index), Box–Muller in f32. */
+/* The CUDA backend's AWGN spec: one Philox block per (noise seed, pair of
+ * global band-sample indices 2p, 2p+1); words 0-1 drive sample 2p and
+ * words 2-3 sample 2p+1, each through Box–Muller in f32. */
 void orc_noise_pair(uint64_t seed, int64_t g, float *z_re, float *z_im) {
     uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
-    uint32_t ctr[4] = {(uint32_t)(uint64_t)g, (uint32_t)((uint64_t)g >> 32), 0x4E4F4953u, 0u};
+    uint64_t p = (uint64_t)g >> 1;
+    uint32_t ctr[4] = {(uint32_t)p, (uint32_t)(p >> 32), 0x4E4F4953u, 0u};
     uint32_t x[4];
     orc_philox4x32_10(ctr, key, x);
-    float u1 = ((float)(x[0] >> 8) + 1.0f) * 0x1.0p-24f;
-    float u2 = (float)(x[1] >> 8) * 0x1.0p-24f;
+    int h = (int)(g & 1) * 2;
+    float u1 = ((float)(x[h] >> 8) + 1.0f) * 0x1.0p-24f;
+    float u2 = (float)(x[h + 1] >> 8) * 0x1.0p-24f;
     float rr = sqrtf(-2.0f * logf(u1));
     float ang = 6.28318548f * u2;
     *z_re = rr * cosf(ang);
