@@ -181,3 +181,21 @@ def test_batch_profiling_times_each_fanout_without_changing_bits(ctx):
     for x, y in zip(got, ref):
         assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
     prep.close()
+
+
+def test_rank_shards_reproduce_the_whole_scene(ctx):
+    """Each rank of a 2-way receiver sharding (run here one after the
+    other on one GPU: the shards share nothing) renders exactly what the
+    single batch over every unit renders."""
+    from lipika_b200 import shard as S
+    prep = P.Prepared(_uneven_scene(), ctx)
+    whole = N.Batch(ctx, _units(prep, N.LPK_SOLVER_SPLIT), round_s=0.25).render()
+    got = {}
+    for rank in range(2):
+        part = S.render_rank_gpu(prep, rank, 2, seed=2026, round_s=0.3)
+        assert not set(part) & set(got)
+        got.update(part)
+    assert sorted(got) == list(range(len(whole)))
+    for w, iq in got.items():
+        assert np.array_equal(iq.view(np.uint32), whole[w].view(np.uint32)), w
+    prep.close()
