@@ -28,7 +28,9 @@ enum NavKind : int32_t { kNavOff = 0, kNavDummy = 1, kNavFull = 2 };
 // One transmitter in device memory. Tables live in the context's scene
 // arena; the trajectory grid is interleaved (x, y, z, pad) per point so a
 // lerp reads one 64-byte line for the two bracketing points.
-struct DevTx {
+// 16-byte aligned so that anything staged after an array of DevTx in
+// shared memory (the 16-byte aligned anchor records) stays aligned.
+struct __align__(16) DevTx {
     int32_t traj_kind, sig_kind, nav_kind, has_repeat;
     int32_t has_gate, gate_n, cw_anchored, reserved;
     double sx, sy, sz;                  // stationary ECEF
@@ -49,6 +51,7 @@ struct DevTx {
     double gate_period, gate_phase;
     const double2 *gate_on;             // (start, end)
 };
+static_assert(sizeof(DevTx) % 16 == 0, "DevTx arrays must keep 16-byte alignment");
 
 // Per-band constants (host-computed where the reference computes them once).
 struct DevBand {

@@ -71,6 +71,7 @@ struct __align__(16) AnchorRec {
     double chip_fl0;                  // C/A: a whole chip count at or below the tile's first chip
     int32_t chip_m0, pad;             // C/A: chip_fl0 mod 1023
 };
+static_assert(sizeof(AnchorRec) % 16 == 0, "AnchorRec arrays must keep 16-byte alignment");
 
 // Lerp position at epoch-relative time t with the segment forced to `lo`
 // (linear extrapolation beyond it), without rounding epoch + t: de is
