@@ -71,6 +71,14 @@ lpk_status lpk_profile_enable(lpk_ctx *ctx, int32_t on);
 lpk_status lpk_profile_reset(lpk_ctx *ctx);
 lpk_status lpk_profile_read(lpk_ctx *ctx, double *fanout_ms, int64_t *fanout_launches,
                             int64_t *all_launches);
+/* Horizon gate counters of this context (src/channel/horizon.rs): with an
+ * antenna cutoff, each block of band samples (256 in the FP64 kernel, one
+ * tile in the split and batched kernels) tests every transmitter with the
+ * reference's certainly_below_cutoff bound and skips those certainly below
+ * the cutoff for all its samples (their contribution is zero either way).
+ * `tested` (block, transmitter) pairs, `skipped` of them; reset != 0
+ * clears both afterwards. */
+lpk_status lpk_gate_stats(lpk_ctx *ctx, int64_t *tested, int64_t *skipped, int32_t reset);
 /* Measured FP64 FMA throughput of the device (TFLOP/s, 2 flops per FMA)
  * from a register-resident DFMA chain kernel timed with CUDA events. */
 lpk_status lpk_probe_fp64_peak(lpk_ctx *ctx, double *tflops);

@@ -112,6 +112,7 @@ lpk_status build_dev_band(lpk_ctx *ctx, const lpk_band_desc *d, int64_t i0, int6
     b.ant_fb = d->ant_fb_db;
     b.ant_cutoff = d->ant_cutoff_deg;
     b.n_post = d->n_post;
+    b.gate_stats = ctx ? ctx->d_gate_stats : nullptr;
     for (int k = 0; k < d->n_post; ++k) {
         const lpk_post_op &op = d->post[k];
         b.post_kind[k] = op.kind;
@@ -300,6 +301,19 @@ lpk_status lpk_profile_read(lpk_ctx *c, double *ms, int64_t *fan, int64_t *all) 
     return LPK_OK;
 }
 
+lpk_status lpk_gate_stats(lpk_ctx *c, int64_t *tested, int64_t *skipped, int32_t reset) {
+    if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
+    cudaSetDevice(c->device);
+    unsigned long long h[2] = {0, 0};
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(h, c->d_gate_stats, sizeof h, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && reset) e = cudaMemset(c->d_gate_stats, 0, sizeof h);
+    if (e != cudaSuccess) return cuda_fail(c, e, "gate statistics");
+    if (tested) *tested = (int64_t)h[0];
+    if (skipped) *skipped = (int64_t)h[1];
+    return LPK_OK;
+}
+
 lpk_status lpk_probe_fp64_peak(lpk_ctx *c, double *tflops) {
     if (!c || !tflops) return fail(c, LPK_EINVAL, "NULL argument");
     cudaSetDevice(c->device);
@@ -340,6 +354,8 @@ lpk_status lpk_ctx_create(lpk_ctx **out, int32_t device) {
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev_start);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev_stop);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_gate_stats, 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(c->d_gate_stats, 0, 2 * sizeof(unsigned long long));
     if (e != cudaSuccess) {
         lpk_status st = cuda_fail(nullptr, e, "stream/event creation");
         lpk_ctx_destroy(c);
@@ -372,6 +388,7 @@ void lpk_ctx_destroy(lpk_ctx *c) {
         cudaEventDestroy(p.second);
     }
     if (c->d_scratch) cudaFree(c->d_scratch);
+    if (c->d_gate_stats) cudaFree(c->d_gate_stats);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
     if (c->ev_start) cudaEventDestroy(c->ev_start);
     if (c->ev_stop) cudaEventDestroy(c->ev_stop);
@@ -427,6 +444,24 @@ lpk_status lpk_scene_upload(lpk_ctx *c, const lpk_tx_desc *tx, int32_t n_tx) {
             if (st) return st;
             d.grid = (const double4 *)p;
             d.grid_n = s.grid_n;
+            {  // path_bounds, src/geometry/precomputed.rs:88-107 (the horizon gate's bounds)
+                double max_seg2 = 0.0, max_r2 = 0.0;
+                bool finite_all = true;
+                for (int64_t k = 0; k < s.grid_n; ++k) {
+                    const double4 q = g[k];
+                    const double r2 = q.x * q.x + q.y * q.y + q.z * q.z;
+                    finite_all &= std::isfinite(r2);
+                    if (r2 > max_r2) max_r2 = r2;
+                    if (k + 1 < s.grid_n) {
+                        const double ex = g[k + 1].x - q.x, ey = g[k + 1].y - q.y, ez = g[k + 1].z - q.z;
+                        const double seg2 = ex * ex + ey * ey + ez * ez;
+                        finite_all &= std::isfinite(seg2);
+                        if (seg2 > max_seg2) max_seg2 = seg2;
+                    }
+                }
+                d.max_speed = finite_all ? std::sqrt(max_seg2) / s.grid_dt_s : std::nan("");
+                d.max_radius = finite_all ? std::sqrt(max_r2) : std::nan("");
+            }
             d.t0 = s.grid_t0_unix;
             d.dt = s.grid_dt_s;
             d.inv_dt = 1.0 / s.grid_dt_s;

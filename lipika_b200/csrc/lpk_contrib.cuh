@@ -72,4 +72,84 @@ __device__ __forceinline__ bool contribution(const DevTx &tx, const DevBand &b, 
     return true;
 }
 
+// Horizon gate (src/channel/horizon.rs:140-215, certainly_below_cutoff):
+// true only if the per-sample path would give every sample of a stretch a
+// zero antenna gain for this transmitter — its arrival elevation below the
+// cutoff throughout. The stretch is given by its epoch-relative UTC sample
+// times [tu_min, tu_max] and a ball (centre, radius) holding every receiver
+// position. The bound: every emission time lies in [tu_min - L, tu_max]
+// (L a light-time bound), so every source position lies in a ball around
+// the position at the middle of that interval whose radius follows from
+// the table's speed bound; the elevation of the ball's centre plus the
+// angular spread of both balls plus 1e-3 deg must clear the cutoff. Any
+// non-finite input answers "not certain".
+__device__ __forceinline__ bool certainly_below_cutoff(const DevTx &tx, double epoch, double tu_min, double tu_max,
+                                                       double cx, double cy, double cz, double orad,
+                                                       double cutoff_deg) {
+    const double cn = sqrt(cx * cx + cy * cy + cz * cz);
+    if (!isfinite(cn) || !isfinite(orad) || !isfinite(tu_min) || !isfinite(tu_max)) return false;
+    double max_speed, max_radius, slack_m;
+    if (tx.traj_kind == 0) {
+        max_speed = 0.0;
+        max_radius = sqrt(tx.sx * tx.sx + tx.sy * tx.sy + tx.sz * tx.sz);
+        slack_m = 0.0;
+    } else {
+        max_speed = tx.max_speed;
+        max_radius = tx.max_radius;
+        slack_m = 1.0;
+    }
+    // each iterate's range is at most |S| (1 + ω⊕Δ) + |O| with Δ <= 100 s
+    const double light = fmax((1.01 * max_radius + cn + orad) / kSpeedOfLight, kEmissionLag);
+    if (!(light <= 100.0)) return false;
+    const double t_mag = fmax(fabs(tu_min), fabs(tu_max));
+    const double lag = light * (1.0 + 1e-9) + 1e-6 + 1e-12 * t_mag;
+    const double t_lo = epoch + (tu_min - lag), t_hi = epoch + tu_max;
+    const double t_mid = t_lo + 0.5 * (t_hi - t_lo);
+    const double half_span = fmax(t_mid - t_lo, t_hi - t_mid);
+    double sx, sy, sz;
+    traj_position(tx, t_mid, sx, sy, sz);
+    const double srad = max_speed * half_span * (1.0 + 1e-9) + slack_m;
+    const double dx = sx - cx, dy = sy - cy, dz = sz - cz;
+    const double range = sqrt(dx * dx + dy * dy + dz * dz);
+    const double rho = srad + orad;
+    if (!(rho < range) || !(orad < cn)) return false;
+    const double se = (dx * cx + dy * cy + dz * cz) / (range * cn);
+    const double deg = 57.2957795130823208767981548141051703;
+    const double el = asin(fmin(fmax(se, -1.0), 1.0)) * deg;
+    const double spread = (asin(rho / range) + asin(orad / cn)) * deg;
+    return el + spread + 1.0e-3 < cutoff_deg;
+}
+
+// Block-wide min / max of two doubles and logical AND of a flag (all
+// threads of the block take part; every thread receives the result).
+// scratch: 3 x 32 doubles of shared memory.
+__device__ __forceinline__ void block_min_max_and(double &lo, double &hi, double &r2, bool &fin, double *scratch) {
+    for (int off = 16; off > 0; off >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, off));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, off));
+        r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, off));
+    }
+    fin = __all_sync(0xffffffffu, fin);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    __syncthreads();
+    if (lane == 0) {
+        scratch[w] = lo;
+        scratch[32 + w] = hi;
+        scratch[64 + w] = fin ? r2 : __longlong_as_double(0x7ff8000000000000LL);  // NaN marks "not finite"
+    }
+    __syncthreads();
+    lo = scratch[0];
+    hi = scratch[32];
+    r2 = scratch[64];
+    fin = !isnan(r2);
+    for (int k = 1; k < nw; ++k) {
+        lo = fmin(lo, scratch[k]);
+        hi = fmax(hi, scratch[32 + k]);
+        const double v = scratch[64 + k];
+        fin = fin && !isnan(v);
+        r2 = fmax(r2, v);
+    }
+    __syncthreads();
+}
+
 }  // namespace lpk

@@ -50,6 +50,8 @@ struct __align__(16) DevTx {
     double cw_omega, cw_phase0;
     double gate_period, gate_phase;
     const double2 *gate_on;             // (start, end)
+    double max_speed, max_radius;       // bounds of the trajectory table (horizon gate): longest
+                                        // segment / dt and largest |P| (NaN if not finite)
 };
 static_assert(sizeof(DevTx) % 16 == 0, "DevTx arrays must keep 16-byte alignment");
 
@@ -73,6 +75,7 @@ struct DevBand {
     int32_t has_antenna, has_cutoff;
     double ant_peak, ant_horizon, ant_fb, ant_cutoff;
     int32_t n_post, reserved;
+    unsigned long long *gate_stats;     // horizon gate counters (tested, skipped) or NULL
     int32_t post_kind[3];
     float post_a[3], post_b[3];         // gain: g | nonlin: k | adc: fs, lsb
 };

@@ -47,6 +47,7 @@ struct lpk_ctx {
     size_t prof_used = 0;
     int64_t launches = 0;
     int split_variant = 0;  // launch shape of the split fan-out (LPK_SPLIT_VARIANTS)
+    unsigned long long *d_gate_stats = nullptr;  // horizon gate: (stretches tested, skipped)
 };
 
 namespace lpk {

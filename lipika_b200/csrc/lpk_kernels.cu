@@ -40,8 +40,34 @@ k_band_reference(const DevBand b, const DevTx *__restrict__ txs, const int32_t *
         tu = __dsub_rn(t_local, delta);         // :927
         band_rx(b, j, ox, oy, oz);
     }
+    // Horizon gate over the block's samples (src/channel/horizon.rs): a
+    // transmitter certainly below the antenna cutoff for all of them is
+    // skipped; the per-sample path would give it zero gain everywhere.
+    __shared__ double red[96];
+    __shared__ unsigned char skip[256];
+    const bool gate = b.has_antenna && b.has_cutoff;
+    if (gate) {
+        double cx, cy, cz;
+        band_rx(b, (int64_t)blockIdx.x * blockDim.x, cx, cy, cz);  // the block's first sample is in the chunk
+        double lo = live ? tu : __longlong_as_double(0x7ff0000000000000LL);
+        double hi = live ? tu : -__longlong_as_double(0x7ff0000000000000LL);
+        const double ex = ox - cx, ey = oy - cy, ez = oz - cz;
+        double r2 = live ? ex * ex + ey * ey + ez * ez : 0.0;
+        bool fin = !live || (isfinite(tu) && isfinite(r2));
+        block_min_max_and(lo, hi, r2, fin, red);
+        for (int k = threadIdx.x; k < n_active; k += blockDim.x) {
+            const bool sk = fin && certainly_below_cutoff(stx[k], b.epoch, lo, hi, cx, cy, cz, sqrt(r2), b.ant_cutoff);
+            skip[k] = sk;
+            if (b.gate_stats) {
+                atomicAdd(b.gate_stats, 1ull);
+                if (sk) atomicAdd(b.gate_stats + 1, 1ull);
+            }
+        }
+        __syncthreads();
+    }
     float acc_re = 0.0f, acc_im = 0.0f;
     for (int k = 0; k < n_active; ++k) {
+        if (gate && skip[k]) continue;  // block-uniform
         float cr = 0.0f, ci = 0.0f;
         bool on = false;
         if (live) {

@@ -496,12 +496,46 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
         // chunk is never stored, not even as a diagnostic)
         fit |= (unsigned)(tu >= tu0 && tu <= tu_hi) << s;
     }
+    // Horizon gate over the tile's samples (src/channel/horizon.rs): with an
+    // antenna cutoff, a transmitter certainly below it for every sample of
+    // the tile adds nothing (the exact path would give it zero gain).
+    __shared__ double gate_red[96];
+    __shared__ unsigned char gate_skip[256];
+    const bool hgate = b.has_antenna && b.has_cutoff;  // uniform over the block
+    if (hgate) {
+        double lo = __longlong_as_double(0x7ff0000000000000LL), hi = -lo, r2 = 0.0;
+        bool fin = true;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            if (!((live >> s) & 1u)) continue;
+            const double tu = __dsub_rn(sc[s].tl, sc[s].dl);
+            fin = fin && isfinite(tu);
+            lo = fmin(lo, tu);
+            hi = fmax(hi, tu);
+        }
+        block_min_max_and(lo, hi, r2, fin, gate_red);
+        for (int k = threadIdx.x; k < n_active; k += blockDim.x) {
+            const bool sk =
+                fin && certainly_below_cutoff(stx[k], b.epoch, lo, hi, b.rx[0], b.rx[1], b.rx[2], 0.0, b.ant_cutoff);
+            gate_skip[k] = sk;
+            if (b.gate_stats) {
+                atomicAdd(b.gate_stats, 1ull);
+                if (sk) atomicAdd(b.gate_stats + 1, 1ull);
+            }
+        }
+        __syncthreads();
+    }
     for (int k = 0; k < n_active; ++k) {
         const AnchorRec &R = srec[k];
+        if (hgate && gate_skip[k]) continue;
+        // gate_off: the transmitter is silent over the tile's fitted span; a
+        // sample outside that span (a clock excursion beyond the fit
+        // margin) is still evaluated exactly
         const bool gate_off = (R.flags & kRecGateOff) != 0;
-        if (gate_off && !DBG) continue;
+        const unsigned outside = live & ~fit;
+        if (gate_off && !DBG && outside == 0) continue;
         const DevTx &T = stx[k];
-        unsigned redo = live;
+        unsigned redo = gate_off ? (DBG ? live : outside) : live;
         if (!(R.flags & kRecExact) && !gate_off) {
             redo = 0;
             const bool kink = R.node0 < kSplitInf || R.node1 < kSplitInf;  // uniform over the block
@@ -533,7 +567,7 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
             double ph = 0.0, te = 0.0, rg = 0.0;
             contribution(T, b, sc[s].tl, __dsub_rn(sc[s].tl, sc[s].dl), sc[s].dl, b.rx[0], b.rx[1], b.rx[2], cr, ci,
                          &ph, &te, &rg);
-            if (!gate_off) {
+            if (!gate_off || ((outside >> s) & 1u)) {
                 ar[s] = __fadd_rn(ar[s], cr);
                 ai[s] = __fadd_rn(ai[s], ci);
             }

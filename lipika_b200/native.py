@@ -118,6 +118,7 @@ SIGNATURES = {
     "lpk_profile_reset": (C.c_int32, [_VP]),
     "lpk_profile_read": (C.c_int32, [_VP, _D, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "lpk_probe_fp64_peak": (C.c_int32, [_VP, _D]),
+    "lpk_gate_stats": (C.c_int32, [_VP, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int32]),
     "lpk_scene_upload": (C.c_int32, [_VP, C.POINTER(TxDesc), C.c_int32]),
     "lpk_band_chunk": (C.c_int32, [_VP, C.POINTER(BandDesc), _I32, C.c_int32, C.c_int64, C.c_int64, _D, _D, _CF, _U8]),
     "lpk_band_chunk_device": (C.c_int32, [_VP, C.POINTER(BandDesc), _I32, C.c_int32, C.c_int64, C.c_int64,
