@@ -67,6 +67,8 @@ def _args():
     p.add_argument("--e2e-round-s", type=float, default=4.0,
                    help="seconds per round of the e2e leg (shorter rounds overlap more of the copy-out)")
     p.add_argument("--no-autotune", action="store_true", help="keep the default split launch shape")
+    p.add_argument("--no-c2", action="store_true",
+                   help="skip the secondary workload (24 C/A x 32 receivers, uneven bands, 30 s)")
     p.add_argument("--variant", type=int, default=-1,
                    help="split launch shape (lpk_split_variant_info) instead of autotuning")
     return p.parse_args()
@@ -426,6 +428,10 @@ def run_ours(a):
                "path": f"lpk_scene_prepare + lpk_generate_scene (C ABI): batched rounds of {a.e2e_round_s} s, "
                        "outputs double-buffered into pinned host memory on a copy stream"}
 
+    c2 = None
+    if ws == 1 and not a.no_c2 and a.solver == "split":
+        c2 = _c2_leg(ctx, L, N, P, timed)
+
     base = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         base, _ = cpu_baseline(a.duration, a.cpu_seconds)
@@ -467,13 +473,63 @@ def run_ours(a):
                              "frac": achieved_gbs / hbm_peak, "peak_source": hbm_src,
                              "algorithmic_bytes_per_launch": BYTES_PER_BAND_SAMPLE * band_per_launch}},
         "e2e": e2e, "gpu_launches": int(all_n.value), "clocks": clk,
-        "plain_fp64": plain, "other_paths": others or None,
+        "plain_fp64": plain, "other_paths": others or None, "secondary_workload": c2,
         "speedup_vs_plain_fp64": (value / plain["value"]) if plain else None,
     }
     if base is not None:
         line["cpu_baseline"] = base
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _c2_leg(ctx, L, N, P, timed, steps=2):
+    """The batching workload: 24 C/A transmitters x 32 receivers with 1-3
+    bands each of 48 kS/s - 4.096 MS/s, 30 s (every transmitter in every
+    band). Batched split path vs the per-band split and plain FP64 kernels,
+    device-resident outputs (per-band launches reuse one output buffer)."""
+    import torch
+    from tests import scenes
+    sc = scenes.config_c2(duration_s=30.0)
+    prep = P.Prepared(sc, ctx)
+    per, total_band, total_txrx = _txrx_counts(prep)
+    units = []
+    for w, (r, b, n, k) in enumerate(per):
+        d = prep.band_desc(r, b, 2026, w)
+        if d.clock_mode == N.LPK_CLOCK_HOST:
+            d.clock_mode = N.LPK_CLOCK_DEVICE_WALK
+        d.solver = N.LPK_SOLVER_SPLIT
+        units.append((d, prep.active(r, b), n))
+    batch = N.Batch(ctx, units, 2.0)
+    batch.autotune(rnd=batch.n_rounds // 2, reps=2)
+    v, bps, _ = batch.config()
+
+    def bstep():
+        ctx.check(L.lpk_batch_reset(batch.h))
+        for r in range(batch.n_rounds):
+            ctx.check(L.lpk_batch_run(batch.h, r))
+    tb = timed(bstep, steps)
+    batch.close()
+    chunk = 1 << 22
+    out = torch.empty(2 * chunk, dtype=torch.float32, device="cuda")
+    acts = [(C.c_int32 * max(len(act), 1))(*act) for (_, act, _) in units]
+
+    def band_step(solver):
+        for (d, act, n), cact in zip(units, acts):
+            d.solver = solver
+            for i0 in range(0, n, chunk):
+                N.check(L.lpk_band_chunk_device(ctx.h, C.byref(d), cact, len(act), i0, min(chunk, n - i0), None,
+                                                None, out.data_ptr(), None), ctx.h)
+    ts = timed(lambda: band_step(N.LPK_SOLVER_SPLIT), steps)
+    tp = timed(lambda: band_step(N.LPK_SOLVER_REFERENCE), 1)
+    prep.close()
+    rate = lambda ms, k: total_txrx * k / (ms * 1e-3)
+    res = {"workload": "c2: 24 C/A x 32 receivers, 1-3 bands each (48 kS/s - 4.096 MS/s), 30 s, AWGN on, "
+                       "device clock walk",
+           "tx_rx_samples_per_step": total_txrx, "work_units": len(units), "unit": UNIT,
+           "batched_split": rate(tb, steps), "split_per_band": rate(ts, steps), "plain_fp64_per_band": rate(tp, 1),
+           "batch_round_s": 2.0, "batch_launch_shape": {"variant": v, "blocks_per_sm": bps}}
+    res["speedup_batched_vs_plain_fp64"] = res["batched_split"] / res["plain_fp64_per_band"]
+    return res
 
 
 def _clone(d, solver):
