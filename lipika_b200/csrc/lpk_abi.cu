@@ -66,6 +66,14 @@ lpk_status ensure_pinned(lpk_ctx *ctx, size_t bytes) {
     return LPK_OK;
 }
 
+cudaError_t pool_alloc(lpk_ctx *ctx, void **p, size_t bytes) {
+    return cudaMallocFromPoolAsync(p, bytes ? bytes : 16, ctx->pool, ctx->stream);
+}
+
+void pool_free(lpk_ctx *ctx, void *p) {
+    if (p) cudaFreeAsync(p, ctx->stream);
+}
+
 static bool finite(double x) { return std::isfinite(x); }
 
 // Lower an lpk_band_desc to the device constants, computing once what the
@@ -354,6 +362,16 @@ lpk_status lpk_ctx_create(lpk_ctx **out, int32_t device) {
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev_start);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev_stop);
+    if (e == cudaSuccess) {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof props);
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        e = cudaMemPoolCreate(&c->pool, &props);
+        uint64_t keep = ~0ull;  // never trim: memory returns to this pool, not to the driver
+        if (e == cudaSuccess) e = cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_gate_stats, 2 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMemset(c->d_gate_stats, 0, 2 * sizeof(unsigned long long));
     if (e != cudaSuccess) {
@@ -366,7 +384,7 @@ lpk_status lpk_ctx_create(lpk_ctx **out, int32_t device) {
 }
 
 static void free_scene(lpk_ctx *c) {
-    for (void *p : c->scene_allocs) cudaFree(p);
+    for (void *p : c->scene_allocs) pool_free(c, p);
     c->scene_allocs.clear();
     c->h_tx.clear();
     c->d_tx = nullptr;
@@ -389,6 +407,10 @@ void lpk_ctx_destroy(lpk_ctx *c) {
     }
     if (c->d_scratch) cudaFree(c->d_scratch);
     if (c->d_gate_stats) cudaFree(c->d_gate_stats);
+    if (c->pool) {
+        cudaStreamSynchronize(c->stream);
+        cudaMemPoolDestroy(c->pool);
+    }
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
     if (c->ev_start) cudaEventDestroy(c->ev_start);
     if (c->ev_stop) cudaEventDestroy(c->ev_stop);
@@ -399,15 +421,13 @@ void lpk_ctx_destroy(lpk_ctx *c) {
 static lpk_status upload_bytes(lpk_ctx *c, const void *src, size_t bytes, void **dst) {
     *dst = nullptr;
     if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMalloc(dst, bytes);
+    cudaError_t e = pool_alloc(c, dst, bytes);
     if (e != cudaSuccess) return fail(c, LPK_ENOMEM, std::string("scene allocation failed: ") + cudaGetErrorString(e));
     c->scene_allocs.push_back(*dst);
-    if (src) {
-        e = cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
-        if (e != cudaSuccess) return cuda_fail(c, e, "scene upload");
-    } else {
-        cudaMemset(*dst, 0, bytes);
-    }
+    // pageable source: the copy has consumed it when the call returns
+    e = src ? cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, c->stream)
+            : cudaMemsetAsync(*dst, 0, bytes, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "scene upload");
     return LPK_OK;
 }
 
@@ -538,6 +558,8 @@ lpk_status lpk_scene_upload(lpk_ctx *c, const lpk_tx_desc *tx, int32_t n_tx) {
     void *p;
     lpk_status st = upload_bytes(c, h.data(), sizeof(DevTx) * h.size(), &p);
     if (st) return st;
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "scene upload");
     c->d_tx = (DevTx *)p;
     c->h_tx = std::move(h);
     c->n_tx = n_tx;

@@ -266,7 +266,7 @@ struct lpk_batch {
 namespace {
 
 lpk_status batch_alloc(lpk_batch *b, void **p, size_t bytes) {
-    cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+    cudaError_t e = pool_alloc(b->ctx, p, bytes);
     if (e != cudaSuccess) return fail(b->ctx, LPK_ENOMEM, std::string("batch allocation failed: ") +
                                                                 cudaGetErrorString(e));
     b->allocs.push_back(*p);
@@ -480,7 +480,7 @@ void lpk_batch_destroy(lpk_batch *b) {
     }
     if (b->copy) cudaStreamSynchronize(b->copy);
     drop_graphs(b);
-    for (void *p : b->allocs) cudaFree(p);
+    for (void *p : b->allocs) pool_free(b->ctx, p);
     for (auto &h : b->h_round)
         if (h) cudaFreeHost(h);
     for (int i = 0; i < 2; ++i)

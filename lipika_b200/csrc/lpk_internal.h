@@ -48,6 +48,10 @@ struct lpk_ctx {
     int64_t launches = 0;
     int split_variant = 0;  // launch shape of the split fan-out (LPK_SPLIT_VARIANTS)
     unsigned long long *d_gate_stats = nullptr;  // horizon gate: (stretches tested, skipped)
+    // stream-ordered pool for scene tables and batch buffers: kept across
+    // scenes and batches, so repeated renders reuse memory without a device
+    // synchronisation per allocation
+    cudaMemPool_t pool = nullptr;
 };
 
 namespace lpk {
@@ -56,6 +60,9 @@ lpk_status fail(lpk_ctx *ctx, lpk_status code, const std::string &msg);
 lpk_status cuda_fail(lpk_ctx *ctx, cudaError_t e, const char *what);
 lpk_status ensure_scratch(lpk_ctx *ctx, size_t bytes);
 lpk_status ensure_pinned(lpk_ctx *ctx, size_t bytes);
+// Allocate / free from the context's pool, ordered on its stream.
+cudaError_t pool_alloc(lpk_ctx *ctx, void **p, size_t bytes);
+void pool_free(lpk_ctx *ctx, void *p);
 lpk_status build_dev_band(lpk_ctx *ctx, const lpk_band_desc *b, int64_t i0, int64_t n, DevBand &out);
 lpk_status check_active(lpk_ctx *ctx, const int32_t *active, int32_t n_active);
 
