@@ -599,7 +599,8 @@ lpk_status lpk_band_chunk_device(lpk_ctx *c, const lpk_band_desc *band, const in
     if (span && (st = prepare_walk(c, band, i0, n, b, (double *)((char *)c->d_scratch + off_eps), span))) return st;
     prof_begin(c);
     if (split)
-        e = launch_band_split(c->split_variant, b, c->d_tx, d_active, n_active, (char *)c->d_scratch + off_recs, (float2 *)d_out,
+        e = launch_band_split(c->split_variant, b, c->d_tx, d_active, n_active, (char *)c->d_scratch + off_recs,
+                              (float2 *)d_out,
                               nullptr, nullptr, nullptr, c->stream);
     else
         e = launch_band_reference(b, c->d_tx, d_active, n_active, (float2 *)d_out, d_uw, c->stream);
@@ -665,7 +666,8 @@ lpk_status lpk_band_chunk(lpk_ctx *c, const lpk_band_desc *band, const int32_t *
     if (span && (st = prepare_walk(c, band, i0, n, b, (double *)(base + off_eps), span))) return st;
     prof_begin(c);
     if (split)
-        e = launch_band_split(c->split_variant, b, c->d_tx, d_active, n_active, base + off_recs, d_out, nullptr, nullptr, nullptr,
+        e = launch_band_split(c->split_variant, b, c->d_tx, d_active, n_active, base + off_recs, d_out, nullptr,
+                              nullptr, nullptr,
                               c->stream);
     else
         e = launch_band_reference(b, c->d_tx, d_active, n_active, d_out, d_uw, c->stream);
@@ -727,7 +729,8 @@ lpk_status lpk_tx_contribution(lpk_ctx *c, const lpk_band_desc *band, int32_t tx
     size_t off_act = 8 * bytes;
     size_t off_eps = off_act + 256;
     size_t off_recs = off_eps + align256(sizeof(double) * (size_t)span);
-    lpk_status s2 = ensure_scratch(c, off_recs + (split ? align256(split_recs_bytes(c->split_variant, i0, n, 1)) : 0) + 256);
+    const size_t recs_bytes = split ? align256(split_recs_bytes(c->split_variant, i0, n, 1)) : 0;
+    lpk_status s2 = ensure_scratch(c, off_recs + recs_bytes + 256);
     if (s2) return s2;
     double *d_delta = (double *)c->d_scratch;
     double *d_rx = d_delta + n;
@@ -748,13 +751,16 @@ lpk_status lpk_tx_contribution(lpk_ctx *c, const lpk_band_desc *band, int32_t tx
     if (split) {
         b.has_noise = 0;  // the contribution alone, as transmitter_contribution_at_receiver returns it
         b.n_post = 0;
-        e = launch_band_split(c->split_variant, b, c->d_tx, (const int32_t *)(base + off_act), 1, base + off_recs, d_out, d_phase, d_te,
+        e = launch_band_split(c->split_variant, b, c->d_tx, (const int32_t *)(base + off_act), 1, base + off_recs,
+                              d_out, d_phase, d_te,
                               d_r, c->stream);
     } else {
         e = launch_tx_contribution(b, c->d_tx, tx, d_out, d_phase, d_te, d_r, c->stream);
     }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, sizeof(float2) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
-    if (e == cudaSuccess && phase_out) e = cudaMemcpyAsync(phase_out, d_phase, bytes, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, d_out, sizeof(float2) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess && phase_out)
+        e = cudaMemcpyAsync(phase_out, d_phase, bytes, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess && t_emit_out) e = cudaMemcpyAsync(t_emit_out, d_te, bytes, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess && range_out) e = cudaMemcpyAsync(range_out, d_r, bytes, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -779,7 +785,8 @@ lpk_status lpk_clock_device_delta(lpk_ctx *c, const lpk_band_desc *band, int64_t
     double *d_out = (double *)c->d_scratch;
     if (span && (st = prepare_walk(c, band, i0, n, b, (double *)((char *)c->d_scratch + off_eps), span))) return st;
     cudaError_t e = launch_band_delta(b, d_out, c->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, d_out, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "device clock");
     return LPK_OK;

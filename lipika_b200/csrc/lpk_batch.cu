@@ -188,7 +188,8 @@ k_batch_fanout(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ 
         cur = ru.unit;
         __syncthreads();
         const int64_t first = (ru.t0 + local) * TILE - ru.i0;
-        split_tile<TILE / THREADS, THREADS, false>(*sb, stx, srec, bu.n_active, first, bu.out[rd->parity], nullptr, nullptr,
+        split_tile<TILE / THREADS, THREADS, false>(*sb, stx, srec, bu.n_active, first, bu.out[rd->parity], nullptr,
+                                                   nullptr,
                                                    nullptr);
         __syncthreads();  // the next stage overwrites the shared tiles
     }
@@ -513,7 +514,8 @@ lpk_status lpk_batch_create(lpk_ctx *c, const lpk_work_unit *wu, int32_t n_units
         uh.n_samples = w.n_samples;
         uh.n_active = w.n_active;
         if (w.n_samples < 0) st = fail(c, LPK_EINVAL, "work unit length must be >= 0");
-        else if (w.band.rx_kind != LPK_RX_STATIONARY) st = fail(c, LPK_ENOTSUP, "batch units need a stationary receiver");
+        else if (w.band.rx_kind != LPK_RX_STATIONARY)
+            st = fail(c, LPK_ENOTSUP, "batch units need a stationary receiver");
         else if (w.band.clock_mode != LPK_CLOCK_DETERMINISTIC && w.band.clock_mode != LPK_CLOCK_DEVICE_WALK)
             st = fail(c, LPK_ENOTSUP, "batch units need a deterministic or device-walk clock");
         else if ((st = build_dev_band(c, &w.band, 0, w.n_samples, h_bands[u]))) {
@@ -596,7 +598,8 @@ lpk_status lpk_batch_create(lpk_ctx *c, const lpk_work_unit *wu, int32_t n_units
         st = batch_alloc(b, &p, sizeof(double) * (size_t)std::max<int64_t>(1, b->walks[w].partial_cap));
         h_walks[w].partial = (double *)p;
         if (!st) st = batch_alloc(b, &p, sizeof(double) * (size_t)total_blocks[w]), h_walks[w].totals = (double *)p;
-        if (!st) st = batch_alloc(b, &p, sizeof(double) * (size_t)(total_blocks[w] + 1)), h_walks[w].carry = (double *)p;
+        if (!st)
+            st = batch_alloc(b, &p, sizeof(double) * (size_t)(total_blocks[w] + 1)), h_walks[w].carry = (double *)p;
         if (!st) st = batch_alloc(b, &p, sizeof(double) * (size_t)(total_blocks[w] / kGroupBlocks + 1)),
                  h_walks[w].gsum = (double *)p;
     }

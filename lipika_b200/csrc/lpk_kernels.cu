@@ -217,7 +217,8 @@ cudaError_t launch_or_flags(const uint32_t *d_uw, uint8_t *d_unocc, int32_t n_ac
 cudaError_t launch_walk_totals(uint64_t seed, double sigma, int64_t b_from, int64_t b_to, double *d_tot,
                                cudaStream_t s) {
     if (b_to <= b_from) return cudaSuccess;
-    k_walk_block<<<(unsigned)(b_to - b_from), kWalkThreads, 0, s>>>(seed, sigma, b_from, d_tot, nullptr, nullptr, 0, -1);
+    k_walk_block<<<(unsigned)(b_to - b_from), kWalkThreads, 0, s>>>(seed, sigma, b_from, d_tot, nullptr, nullptr, 0,
+                                                                     -1);
     return cudaGetLastError();
 }
 

@@ -654,7 +654,8 @@ lpk_status lpk_mlp_loss_grad(lpk_mlp *m, const float *x, const float *t, int64_t
     lpk_ctx *c = m->ctx;
     if (n <= 0 || !x || !t) return fail(c, LPK_EINVAL, "bad gradient arguments");
     cudaSetDevice(c->device);
-    const size_t bx = (sizeof(float) * (size_t)n * kF + 255) / 256 * 256, bt = (sizeof(float) * (size_t)n + 255) / 256 * 256;
+    const size_t bx = (sizeof(float) * (size_t)n * kF + 255) / 256 * 256;
+    const size_t bt = (sizeof(float) * (size_t)n + 255) / 256 * 256;
     lpk_status s = ensure_scratch(c, bx + bt + 256);
     if (s) return s;
     float *d_x = (float *)c->d_scratch, *d_t = (float *)((char *)c->d_scratch + bx);
@@ -709,7 +710,8 @@ lpk_status lpk_mlp_fit(lpk_mlp *m, int32_t tx, const double *rx, double epoch, d
     std::vector<float> hx((size_t)n_train * kF), hy((size_t)n_train);
     int32_t bad = 0;
     cudaError_t e = cudaMemcpyAsync(hx.data(), d_x, sizeof(float) * hx.size(), cudaMemcpyDeviceToHost, c->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(hy.data(), d_y, sizeof(float) * hy.size(), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hy.data(), d_y, sizeof(float) * hy.size(), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) {
@@ -776,7 +778,8 @@ lpk_status lpk_solve_converged(lpk_ctx *c, int32_t tx, const double *rx, double 
     if (scheme != LPK_ITER_FIXED_POINT && scheme != LPK_ITER_NEWTON) return fail(c, LPK_EINVAL, "unknown scheme");
     if (start != LPK_START_LAG && start != LPK_START_GEOMETRIC && start != LPK_START_LEARNED)
         return fail(c, LPK_EINVAL, "unknown start");
-    if (start == LPK_START_LEARNED && (!m || m->ctx != c)) return fail(c, LPK_EINVAL, "learned start needs an mlp of this context");
+    if (start == LPK_START_LEARNED && (!m || m->ctx != c))
+        return fail(c, LPK_EINVAL, "learned start needs an mlp of this context");
     if (!(tol_s >= 0.0) || max_iter < 1) return fail(c, LPK_EINVAL, "tol must be >= 0 and max_iter >= 1");
     if (n == 0) return LPK_OK;
     cudaSetDevice(c->device);
@@ -806,8 +809,10 @@ lpk_status lpk_solve_converged(lpk_ctx *c, int32_t tx, const double *rx, double 
                                                    m ? m->norm[2 * kF + 1] : 1.0f, d_o, d_i, start_err ? d_e : nullptr);
     c->launches += 1;
     cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(t_emit, d_o, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(iters, d_i, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(t_emit, d_o, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(iters, d_i, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess && start_err)
         e = cudaMemcpyAsync(start_err, d_e, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);

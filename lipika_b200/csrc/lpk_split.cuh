@@ -542,11 +542,11 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
 #define LPK_PASS(KIND)                                                                                           \
     do {                                                                                                         \
         if (kink)                                                                                                \
-            split_pass<KIND, DBG, true, S, THREADS>(T, R, b.epoch, sc, fit & live, ar, ai, redo, first, dbg_phase,      \
-                                                    dbg_temit, dbg_delay);                                       \
+            split_pass<KIND, DBG, true, S, THREADS>(T, R, b.epoch, sc, fit & live, ar, ai, redo, first,        \
+                                                    dbg_phase, dbg_temit, dbg_delay);                            \
         else                                                                                                     \
-            split_pass<KIND, DBG, false, S, THREADS>(T, R, b.epoch, sc, fit & live, ar, ai, redo, first, dbg_phase,     \
-                                                     dbg_temit, dbg_delay);                                      \
+            split_pass<KIND, DBG, false, S, THREADS>(T, R, b.epoch, sc, fit & live, ar, ai, redo, first,       \
+                                                     dbg_phase, dbg_temit, dbg_delay);                           \
     } while (0)
             switch (pass_kind(T, R)) {
             case kPassCa: LPK_PASS(kPassCa); break;
