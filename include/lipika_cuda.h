@@ -265,8 +265,8 @@ int32_t lpk_ctx_split_variant(const lpk_ctx *ctx);
  * Units need a stationary receiver (rx_kind LPK_RX_STATIONARY) and a clock
  * mode of LPK_CLOCK_DETERMINISTIC or LPK_CLOCK_DEVICE_WALK; units whose
  * clock seed, master rate and Allan deviation agree share one walk (the
- * bands of one receiver). Units with solver LPK_SOLVER_REFERENCE or an
- * antenna take the reference-exact path for every sample. */
+ * bands of one receiver). Units with solver LPK_SOLVER_REFERENCE take the
+ * reference-exact path for every sample. */
 typedef struct lpk_batch lpk_batch;
 typedef struct lpk_work_unit {
     lpk_band_desc band;
@@ -412,7 +412,7 @@ enum {
     LPK_GEN_DEVICE_CLOCK = 2,   /* white-FM walk generated on the GPU (counter-based,
                                    moment-matched) instead of the host stream */
     LPK_GEN_SPLIT = 4           /* split-precision fan-out (LPK_SOLVER_SPLIT) where the
-                                   band allows it (stationary receiver, no antenna) */
+                                   band allows it (stationary receiver) */
 };
 
 /* generate_band (src/pipeline.rs:836-1019) on the GPU: the chunk loop with

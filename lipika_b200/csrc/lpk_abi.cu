@@ -598,10 +598,11 @@ lpk_status lpk_band_chunk_device(lpk_ctx *c, const lpk_band_desc *band, const in
     if (e != cudaSuccess) return cuda_fail(c, e, "chunk setup");
     if (span && (st = prepare_walk(c, band, i0, n, b, (double *)((char *)c->d_scratch + off_eps), span))) return st;
     prof_begin(c);
-    if (split)
+    if (split) {
+        b.unocc_words = b.has_antenna ? d_uw : nullptr;
         e = launch_band_split(c->split_variant, b, c->d_tx, d_active, n_active, (char *)c->d_scratch + off_recs,
-                              (float2 *)d_out,
-                              nullptr, nullptr, nullptr, c->stream);
+                              (float2 *)d_out, nullptr, nullptr, nullptr, c->stream);
+    }
     else
         e = launch_band_reference(b, c->d_tx, d_active, n_active, (float2 *)d_out, d_uw, c->stream);
     prof_end(c);
@@ -665,10 +666,11 @@ lpk_status lpk_band_chunk(lpk_ctx *c, const lpk_band_desc *band, const int32_t *
     b.rxpos = d_rx;
     if (span && (st = prepare_walk(c, band, i0, n, b, (double *)(base + off_eps), span))) return st;
     prof_begin(c);
-    if (split)
+    if (split) {
+        b.unocc_words = b.has_antenna ? d_uw : nullptr;
         e = launch_band_split(c->split_variant, b, c->d_tx, d_active, n_active, base + off_recs, d_out, nullptr,
-                              nullptr, nullptr,
-                              c->stream);
+                              nullptr, nullptr, c->stream);
+    }
     else
         e = launch_band_reference(b, c->d_tx, d_active, n_active, d_out, d_uw, c->stream);
     prof_end(c);

@@ -523,7 +523,7 @@ lpk_status lpk_batch_create(lpk_ctx *c, const lpk_work_unit *wu, int32_t n_units
         }
         if (st) break;
         uh.round_len = std::max<int64_t>(1, std::llround(round_s * w.band.fs_hz));
-        uh.exact_only = !(w.band.solver == LPK_SOLVER_SPLIT) || w.band.has_antenna;
+        uh.exact_only = !(w.band.solver == LPK_SOLVER_SPLIT);
         if (w.band.clock_mode == LPK_CLOCK_DEVICE_WALK) {
             const double sigma = w.band.clock_allan_1s / std::sqrt(w.band.clock_master_rate_hz);
             int found = -1;

@@ -76,6 +76,8 @@ struct DevBand {
     double ant_peak, ant_horizon, ant_fb, ant_cutoff;
     int32_t n_post, reserved;
     unsigned long long *gate_stats;     // horizon gate counters (tested, skipped) or NULL
+    uint32_t *unocc_words;              // split kernel: per active transmitter, set when any sample
+                                        // has a non-zero antenna gain (NULL: not reported)
     int32_t post_kind[3];
     float post_a[3], post_b[3];         // gain: g | nonlin: k | adc: fs, lsb
 };
@@ -247,8 +249,10 @@ __device__ __forceinline__ float2 baseband(const DevTx &tx, double t) {
 
 // Antenna::amplitude_at after the elevation geometry of
 // accumulate_reporting_occlusion (channel/mod.rs:190-203, rx/mod.rs:48-58).
-__device__ __forceinline__ float antenna_gain(const DevTx &tx, const DevBand &b, double t_emit_abs,
-                                              double ox, double oy, double oz) {
+// Arrival elevation (degrees) of the source at absolute emission time
+// t_emit_abs seen from O, against the geocentric up O/|O|.
+__device__ __forceinline__ double antenna_elevation(const DevTx &tx, double t_emit_abs, double ox, double oy,
+                                                   double oz) {
     double sx, sy, sz;
     traj_position_batch(tx, t_emit_abs, sx, sy, sz);
     double on = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(ox, ox), __dmul_rn(oy, oy)), __dmul_rn(oz, oz)));
@@ -257,12 +261,21 @@ __device__ __forceinline__ float antenna_gain(const DevTx &tx, const DevBand &b,
     double se = __ddiv_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, ox), __dmul_rn(dy, oy)), __dmul_rn(dz, oz)),
                           __dmul_rn(dn, on));
     se = se < -1.0 ? -1.0 : (se > 1.0 ? 1.0 : se);
-    double el = __dmul_rn(asin(se), 57.2957795130823208767981548141051703);
+    return __dmul_rn(asin(se), 57.2957795130823208767981548141051703);
+}
+
+// Antenna::amplitude_at (src/rx/mod.rs:48-58) at elevation el (degrees).
+__device__ __forceinline__ float antenna_pattern(const DevBand &b, double el) {
     if (b.has_cutoff && el < b.ant_cutoff) return 0.0f;
     double dbi = (el >= 0.0)
                      ? __dadd_rn(b.ant_horizon, __dmul_rn(__dsub_rn(b.ant_peak, b.ant_horizon), __ddiv_rn(el, 90.0)))
                      : __dsub_rn(b.ant_horizon, b.ant_fb);
     return (float)pow(10.0, __ddiv_rn(dbi, 20.0));
+}
+
+__device__ __forceinline__ float antenna_gain(const DevTx &tx, const DevBand &b, double t_emit_abs,
+                                              double ox, double oy, double oz) {
+    return antenna_pattern(b, antenna_elevation(tx, t_emit_abs, ox, oy, oz));
 }
 
 // ---------------------------------------------------------------- noise

@@ -82,9 +82,9 @@ size_t split_recs_bytes(int variant, int64_t i0, int64_t n, int32_t n_active);
 cudaError_t launch_band_split(int variant, const DevBand &b, const DevTx *d_tx, const int32_t *d_active,
                               int32_t n_active, void *d_recs, float2 *d_out, double *dbg_phase, double *dbg_temit,
                               double *dbg_delay, cudaStream_t s);
-// True when the band can take the split path (stationary receiver, no antenna).
+// True when the band can take the split path (stationary receiver).
 inline bool use_split(const lpk_band_desc *d) {
-    return d->solver == LPK_SOLVER_SPLIT && d->rx_kind == LPK_RX_STATIONARY && !d->has_antenna;
+    return d->solver == LPK_SOLVER_SPLIT && d->rx_kind == LPK_RX_STATIONARY;
 }
 cudaError_t launch_or_flags(const uint32_t *d_uw, uint8_t *d_unocc, int32_t n_active, int mode, cudaStream_t s);
 // Totals of scan blocks [b_from, b_to).

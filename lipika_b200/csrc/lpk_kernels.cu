@@ -242,7 +242,7 @@ cudaError_t launch_band_reference(const DevBand &b, const DevTx *d_tx, const int
                                   int32_t n_active, float2 *d_out, uint32_t *d_unocc, cudaStream_t s) {
     if (b.n <= 0) return cudaSuccess;
     size_t smem = sizeof(DevTx) * (size_t)n_active;
-    if (smem > 48 * 1024) {
+    if (smem > 40 * 1024) {  // leaves room for the kernel's static shared arrays
         cudaError_t e = cudaFuncSetAttribute(k_band_reference, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;

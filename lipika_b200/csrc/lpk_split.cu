@@ -85,7 +85,7 @@ cudaError_t launch_band_split(int variant, const DevBand &b, const DevTx *d_tx, 
     }
     const size_t smem = (sizeof(DevTx) + sizeof(AnchorRec)) * (size_t)n_active;
     SplitKernel kern = dbg_phase ? sh.dbg : sh.fast;
-    if (smem > 48 * 1024) {
+    if (smem > 40 * 1024) {  // leaves room for the kernel's static shared arrays
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }

@@ -5,8 +5,8 @@
 // two things the split path reproduces explicitly:
 //  * the lerp table is piecewise linear in time, so each iterate has a slope
 //    kink where its query time crosses a 10 ms grid node: every tile is fitted
-//    per segment (pieces A and B) and a sample picks its piece from its own
-//    query time;
+//    per segment (up to four pieces, i.e. tiles up to three grid steps long)
+//    and a sample picks its piece from its own query time;
 //  * each iterate queries the trajectory at the absolute time epoch + t,
 //    which FP64 rounds to ~238 ns: the reference's delay is a fine staircase.
 //    The fits are of the unrounded delay; per sample the exact rounding
@@ -38,6 +38,7 @@ namespace lpk {
     X(4, 1024, 256, 2)        \
     X(5, 1024, 512, 1)
 constexpr int kSplitVariants = 6;
+constexpr int kSplitNodes = 3;  // grid nodes an iterate's query may cross inside one tile
 constexpr int kSplitMaxTile = 1024;
 constexpr int kSplitMinTile = 512;
 // Tiles are aligned to absolute band-sample indices and fitted over a tu range
@@ -56,10 +57,13 @@ enum : int32_t { kRecExact = 1, kRecNavVary = 2, kRecGateOff = 4, kRecCaWide = 8
 
 struct __align__(16) AnchorRec {
     double tu0, tu_hi;                // fit range; Δ origin tu0
-    double node0, node1;              // absolute query time where piece B starts (first / second iterate)
-    double p0a[3], p0b[3];            // first-iterate delay pieces (unrounded query)
-    double p1a[3], p1b[3];            // second-iterate delay pieces (unrounded query)
-    double k0, k1a, k1b;              // ∂delay/∂(query time) per piece
+    // An iterate's query crosses up to kSplitNodes grid nodes inside a tile
+    // (a tile up to 3 grid steps long): piece p >= 1 starts at node[p - 1]
+    // (absolute query time, kSplitInf when absent).
+    double node0[kSplitNodes], node1[kSplitNodes];
+    double p0[kSplitNodes + 1][3];    // first-iterate delay pieces (unrounded query)
+    double p1[kSplitNodes + 1][3];    // second-iterate delay pieces (unrounded query)
+    double k0, k1[kSplitNodes + 1];   // ∂delay/∂(query time): first iterate, second iterate per piece
     double tie;                       // guard on a rounding tie of the second query (s)
     double ulp_q;                     // ulp of the absolute query time
     double tau_if;                    // 2π (f_tx - f_lo)
@@ -172,12 +176,15 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
     const double de = tx.traj_kind != 0 ? b.epoch - tx.t0 : 0.0;
     r.tu0 = tus;
     r.tu_hi = tue;
-    r.node0 = r.node1 = kSplitInf;
+    for (int i = 0; i < kSplitNodes; ++i) r.node0[i] = r.node1[i] = kSplitInf;
     r.tau_if = kTau * (tx.carrier - b.lo);
     r.flags = 0;
     r.nav_pm = 1;
-    r.k0 = r.k1a = r.k1b = 0.0;
-    for (int i = 0; i < 3; ++i) r.p0a[i] = r.p0b[i] = r.p1a[i] = r.p1b[i] = 0.0;
+    r.k0 = 0.0;
+    for (int p = 0; p <= kSplitNodes; ++p) {
+        r.k1[p] = 0.0;
+        for (int i = 0; i < 3; ++i) r.p0[p][i] = r.p1[p][i] = 0.0;
+    }
     int64_t lo0s = 0, lo0e = 0, lo1s = 0, lo1e = 0;
     bool exact = exact_only;
     r.chip_fl0 = 0.0;
@@ -197,44 +204,69 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
         double d0e = iterate_unrounded(tx, tue, tue - kEmissionLag, de, lo0e, ox, oy, oz, b.inv_c, nullptr, nullptr);
         lo1s = seg_unrounded(tx, tus - d0s, de, c3);
         lo1e = seg_unrounded(tx, tue - d0e, de, c4);
-        exact = c1 || c2 || c3 || c4 || lo0e < lo0s || lo0e > lo0s + 1 || lo1e < lo1s || lo1e > lo1s + 1;
-        if (lo0e != lo0s) r.node0 = tx.t0 + (double)lo0e * tx.dt;
-        if (lo1e != lo1s) r.node1 = tx.t0 + (double)lo1e * tx.dt;
+        exact = c1 || c2 || c3 || c4 || lo0e < lo0s || lo0e > lo0s + kSplitNodes || lo1e < lo1s ||
+                lo1e > lo1s + kSplitNodes;
+        for (int i = 0; i < kSplitNodes; ++i) {
+            if (lo0s + i < lo0e) r.node0[i] = tx.t0 + (double)(lo0s + i + 1) * tx.dt;
+            if (lo1s + i < lo1e) r.node1[i] = tx.t0 + (double)(lo1s + i + 1) * tx.dt;
+        }
     }
     double rs = 1.0, re = 1.0, te_s = tus, te_e = tue;
     if (!exact) {
+        // Each piece fits the iterate with its segment forced (the lerp
+        // extrapolated linearly), over the whole tile: smooth, so a
+        // quadratic through three points holds it well below 1 ps.
         double v[3];
-        for (int piece = 0; piece < 2; ++piece) {
-            int64_t lo = piece ? lo0e : lo0s;
-            if (piece && lo0e == lo0s) break;
+        for (int64_t p = 0; p <= lo0e - lo0s; ++p) {
             for (int i = 0; i < 3; ++i) {
                 double tu = tus + i * h;
-                v[i] = iterate_unrounded(tx, tu, tu - kEmissionLag, de, lo, ox, oy, oz, b.inv_c, nullptr, nullptr);
+                v[i] = iterate_unrounded(tx, tu, tu - kEmissionLag, de, lo0s + p, ox, oy, oz, b.inv_c, nullptr,
+                                         nullptr);
             }
-            quad3(v[0], v[1], v[2], h, piece ? r.p0b : r.p0a);
+            quad3(v[0], v[1], v[2], h, r.p0[p]);
         }
-        for (int piece = 0; piece < 2; ++piece) {
-            int64_t lo = piece ? lo1e : lo1s;
-            if (piece && lo1e == lo1s) break;
+        for (int64_t p = 0; p <= lo1e - lo1s; ++p) {
             for (int i = 0; i < 3; ++i)
-                v[i] = solve_unrounded(tx, tus + i * h, de, lo, ox, oy, oz, b.inv_c, nullptr, nullptr);
-            quad3(v[0], v[1], v[2], h, piece ? r.p1b : r.p1a);
+                v[i] = solve_unrounded(tx, tus + i * h, de, lo1s + p, ox, oy, oz, b.inv_c, nullptr, nullptr);
+            quad3(v[0], v[1], v[2], h, r.p1[p]);
         }
-        // ∂delay/∂(query time) of each piece at the tile middle
+        // ∂delay/∂(query time) at the tile middle: the first iterate on its
+        // natural segment, the second per piece
         bool cl;
         const double mid = tus + h;
         const double tq0 = mid - kEmissionLag;
         double d0m = iterate_unrounded(tx, mid, tq0, de, seg_unrounded(tx, tq0, de, cl), ox, oy, oz, b.inv_c,
                                        nullptr, &r.k0);
-        iterate_unrounded(tx, mid, mid - d0m, de, lo1s, ox, oy, oz, b.inv_c, nullptr, &r.k1a);
-        r.k1b = r.k1a;
-        if (lo1e != lo1s) iterate_unrounded(tx, mid, mid - d0m, de, lo1e, ox, oy, oz, b.inv_c, nullptr, &r.k1b);
+        for (int64_t p = 0; p <= lo1e - lo1s; ++p)
+            iterate_unrounded(tx, mid, mid - d0m, de, lo1s + p, ox, oy, oz, b.inv_c, nullptr, &r.k1[p]);
         solve_unrounded(tx, tus, de, lo1s, ox, oy, oz, b.inv_c, nullptr, &rs);
         solve_unrounded(tx, tue, de, lo1e, ox, oy, oz, b.inv_c, nullptr, &re);
-        te_s = tus - poly2(r.p1a, 0.0);
-        te_e = tue - poly2(lo1e != lo1s ? r.p1b : r.p1a, 2.0 * h);
+        te_s = tus - poly2(r.p1[0], 0.0);
+        te_e = tue - poly2(r.p1[lo1e - lo1s], 2.0 * h);
     }
-    const float amp_s = (float)(tx.amp_factor / rs), amp_e = (float)(tx.amp_factor / re);
+    float amp_s = (float)(tx.amp_factor / rs), amp_e = (float)(tx.amp_factor / re);
+    if (!exact && b.has_antenna) {
+        // Antenna gain (src/channel/mod.rs:190-203) folded into the tile's
+        // linear amplitude: the elevation is smooth over a tile; a tile
+        // whose elevation range (three points, 1e-3 deg margin) touches a
+        // discontinuity of the pattern (0 deg, the cutoff) takes the exact
+        // path, one entirely below the cutoff is silent.
+        const double tm = tus + h;
+        const double te_m = tm - solve_unrounded(tx, tm, de, -1, ox, oy, oz, b.inv_c, nullptr, nullptr);
+        const double el_s = antenna_elevation(tx, b.epoch + te_s, ox, oy, oz);
+        const double el_m = antenna_elevation(tx, b.epoch + te_m, ox, oy, oz);
+        const double el_e = antenna_elevation(tx, b.epoch + te_e, ox, oy, oz);
+        const double lo = fmin(fmin(el_s, el_m), el_e) - 1.0e-3, hi = fmax(fmax(el_s, el_m), el_e) + 1.0e-3;
+        if (!(lo == lo) || !(hi == hi) || (lo <= 0.0 && hi >= 0.0) ||
+            (b.has_cutoff && lo <= b.ant_cutoff && hi >= b.ant_cutoff)) {
+            exact = true;
+        } else if (b.has_cutoff && hi < b.ant_cutoff) {
+            r.flags |= kRecGateOff;
+        } else {
+            amp_s = __fmul_rn(amp_s, antenna_pattern(b, el_s));
+            amp_e = __fmul_rn(amp_e, antenna_pattern(b, el_e));
+        }
+    }
     r.amp0 = amp_s;
     r.amp1 = (tue > tus) ? (amp_e - amp_s) / (float)(tue - tus) : 0.0f;
     r.guard = ldexp(16.0, ilogb(fmax(fmax(fabs(te_s), fabs(te_e)), 1.0)) - 52);
@@ -399,12 +431,13 @@ template <int K, bool DBG, bool KINK, int S, int THREADS>
 __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, double epoch, const SampleCtx *sc,
                                            unsigned fit, float *ar, float *ai, unsigned &redo, int64_t first,
                                            double *dbg_phase, double *dbg_temit, double *dbg_delay) {
-    const double tu0 = R.tu0, node0 = R.node0, node1 = R.node1, k0 = R.k0, tie = R.tie;
+    const double tu0 = R.tu0, k0 = R.k0, tie = R.tie;
     const double half = 0.5 * R.ulp_q, tau_if = R.tau_if, nts = tx.neg_tau_src, guard = R.guard;
     const float amp0 = R.amp0, amp1 = R.amp1;
     // one piece per iterate (no grid node inside the tile): coefficients in registers
-    const double a0 = R.p0a[0], a1 = R.p0a[1], a2 = R.p0a[2], b0 = R.p1a[0], b1 = R.p1a[1], b2 = R.p1a[2];
-    const double ka = R.k1a;
+    const double a0 = R.p0[0][0], a1 = R.p0[0][1], a2 = R.p0[0][2];
+    const double b0 = R.p1[0][0], b1 = R.p1[0][1], b2 = R.p1[0][2];
+    const double ka = R.k1[0];
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         const SampleCtx &c = sc[s];
@@ -412,7 +445,9 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
         const double d = tu - tu0;
         double t1s, poly1, k1;
         if constexpr (KINK) {
-            const double *p0 = __dadd_rn(epoch, __dsub_rn(tu, kEmissionLag)) >= node0 ? R.p0b : R.p0a;
+            const double q = __dadd_rn(epoch, __dsub_rn(tu, kEmissionLag));
+            const int i0 = (q >= R.node0[0]) + (q >= R.node0[1]) + (q >= R.node0[2]);
+            const double *p0 = R.p0[i0];
             t1s = tu - fma(d, fma(d, p0[2], p0[1]), p0[0]);
         } else {
             t1s = tu - fma(d, fma(d, a2, a1), a0);
@@ -422,10 +457,10 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
         const double e1 = __dsub_rn(s1, epoch);
         bool ok = fabs(fabs(e1 - t1r) - half) > tie;
         if constexpr (KINK) {
-            const bool pb = s1 >= node1;
-            const double *p1 = pb ? R.p1b : R.p1a;
+            const int i1 = (s1 >= R.node1[0]) + (s1 >= R.node1[1]) + (s1 >= R.node1[2]);
+            const double *p1 = R.p1[i1];
             poly1 = fma(d, fma(d, p1[2], p1[1]), p1[0]);
-            k1 = pb ? R.k1b : R.k1a;
+            k1 = R.k1[i1];
         } else {
             poly1 = fma(d, fma(d, b2, b1), b0);
             k1 = ka;
@@ -538,7 +573,7 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
         unsigned redo = gate_off ? (DBG ? live : outside) : live;
         if (!(R.flags & kRecExact) && !gate_off) {
             redo = 0;
-            const bool kink = R.node0 < kSplitInf || R.node1 < kSplitInf;  // uniform over the block
+            const bool kink = R.node0[0] < kSplitInf || R.node1[0] < kSplitInf;  // uniform over the block
 #define LPK_PASS(KIND)                                                                                           \
     do {                                                                                                         \
         if (kink)                                                                                                \
@@ -558,6 +593,8 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
             }
 #undef LPK_PASS
             redo &= live;
+            if (b.unocc_words && __any_sync(0xffffffffu, (fit & live) != 0) && (threadIdx.x & 31) == 0)
+                atomicOr(b.unocc_words + k, 1u);  // the tile's gain is non-zero throughout
         }
         if (redo == 0) continue;
 #pragma unroll
@@ -565,8 +602,9 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
             if (!((redo >> s) & 1u)) continue;
             float cr = 0.0f, ci = 0.0f;
             double ph = 0.0, te = 0.0, rg = 0.0;
-            contribution(T, b, sc[s].tl, __dsub_rn(sc[s].tl, sc[s].dl), sc[s].dl, b.rx[0], b.rx[1], b.rx[2], cr, ci,
-                         &ph, &te, &rg);
+            const bool on = contribution(T, b, sc[s].tl, __dsub_rn(sc[s].tl, sc[s].dl), sc[s].dl, b.rx[0], b.rx[1],
+                                         b.rx[2], cr, ci, &ph, &te, &rg);
+            if (on && b.unocc_words && !gate_off) atomicOr(b.unocc_words + k, 1u);
             if (!gate_off || ((outside >> s) & 1u)) {
                 ar[s] = __fadd_rn(ar[s], cr);
                 ai[s] = __fadd_rn(ai[s], ci);

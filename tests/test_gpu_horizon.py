@@ -67,7 +67,7 @@ def test_gate_in_the_batch_changes_no_bit(ctx):
     for w, (r, b) in enumerate(prep.work()):
         d = prep.band_desc(r, b, 7, w)
         d.clock_mode = N.LPK_CLOCK_DEVICE_WALK
-        d.solver = N.LPK_SOLVER_SPLIT  # antenna bands take the exact path inside the batch
+        d.solver = N.LPK_SOLVER_SPLIT
         units.append((d, prep.active(r, b), prep.n_samples(r, b)))
     single = []
     for d, act, n in units:
