@@ -128,7 +128,7 @@ k_batch_carry(const DevWalk *__restrict__ walks, const RoundDesc *__restrict__ r
 __global__ void __launch_bounds__(128)
 k_batch_anchor(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ units,
                const DevTx *__restrict__ txs, const int32_t *__restrict__ act, const RoundDesc *__restrict__ rd,
-               AnchorRec *__restrict__ recs) {
+               AnchorRec *__restrict__ recs, AnchorExt *__restrict__ exts) {
     const int64_t total = rd->total_recs;
     const int tile_len = rd->tile;
     for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < total;
@@ -141,8 +141,10 @@ k_batch_anchor(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ 
         const int k = (int)(local - tile * bu.n_active);
         const int64_t gs = (ru.t0 + tile) * tile_len;
         AnchorRec r;
-        fit_anchor(bands[ru.unit], txs[act[bu.act_off + k]], gs, gs + tile_len - 1, bu.exact_only != 0, r);
+        AnchorExt x;
+        fit_anchor(bands[ru.unit], txs[act[bu.act_off + k]], gs, gs + tile_len - 1, bu.exact_only != 0, r, x);
         recs[id] = r;
+        if (r.n_nodes > 1) exts[id] = x;
     }
 }
 
@@ -154,7 +156,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
 k_batch_fanout(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ units,
                const DevTx *__restrict__ txs, const int32_t *__restrict__ act, const DevWalk *__restrict__ walks,
                const RoundDesc *__restrict__ rd, const AnchorRec *__restrict__ recs,
-               unsigned long long *__restrict__ counter, int32_t max_active) {
+               const AnchorExt *__restrict__ exts, unsigned long long *__restrict__ counter, int32_t max_active) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     DevBand *sb = reinterpret_cast<DevBand *>(smem_raw);
     DevTx *stx = reinterpret_cast<DevTx *>(smem_raw + ((sizeof(DevBand) + 15) / 16) * 16);
@@ -188,15 +190,16 @@ k_batch_fanout(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ 
         cur = ru.unit;
         __syncthreads();
         const int64_t first = (ru.t0 + local) * TILE - ru.i0;
-        split_tile<TILE / THREADS, THREADS, false>(*sb, stx, srec, bu.n_active, first, bu.out[rd->parity], nullptr,
-                                                   nullptr,
+        split_tile<TILE / THREADS, THREADS, false, false>(*sb, stx, srec, exts + ru.rec_off + local * bu.n_active,
+                                                          bu.n_active, first, bu.out[rd->parity], nullptr, nullptr,
                                                    nullptr);
         __syncthreads();  // the next stage overwrites the shared tiles
     }
 }
 
 using FanoutKernel = void (*)(const DevBand *, const BatchUnit *, const DevTx *, const int32_t *, const DevWalk *,
-                              const RoundDesc *, const AnchorRec *, unsigned long long *, int32_t);
+                              const RoundDesc *, const AnchorRec *, const AnchorExt *, unsigned long long *,
+                              int32_t);
 
 struct FanoutShape {
     int tile, threads;
@@ -249,6 +252,7 @@ struct lpk_batch {
     cudaEvent_t fork = nullptr, join = nullptr;
     cudaEvent_t mark[2] = {nullptr, nullptr};       // placeholders of the profiling event nodes
     AnchorRec *d_recs = nullptr;
+    AnchorExt *d_exts = nullptr;
     unsigned long long *d_counter = nullptr;
     int64_t recs_cap = 0;
     int64_t n_rounds = 0;
@@ -383,7 +387,7 @@ lpk_status build_graph(lpk_batch *b, int p) {
     cudaEventRecord(b->fork, c->stream);
     cudaStreamWaitEvent(b->side, b->fork, 0);
     k_batch_anchor<<<b->anchor_grid, 128, 0, b->side>>>(b->d_bands, b->d_units, c->d_tx, b->d_act, b->d_round,
-                                                        b->d_recs);
+                                                        b->d_recs, b->d_exts);
     cudaEventRecord(b->join, b->side);
     if (!b->walks.empty()) {
         k_batch_walk<<<b->walk_grid, kWalkThreads, 0, c->stream>>>(b->d_walks, b->d_round);
@@ -393,7 +397,8 @@ lpk_status build_graph(lpk_batch *b, int p) {
     cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), c->stream);
     if (prof) cudaEventRecordWithFlags(b->mark[0], c->stream, cudaEventRecordExternal);
     sh.kern<<<(unsigned)(dev_sms * b->bps), sh.threads, smem, c->stream>>>(
-        b->d_bands, b->d_units, c->d_tx, b->d_act, b->d_walks, b->d_round, b->d_recs, b->d_counter, b->max_active);
+        b->d_bands, b->d_units, c->d_tx, b->d_act, b->d_walks, b->d_round, b->d_recs, b->d_exts, b->d_counter,
+        b->max_active);
     if (prof) cudaEventRecordWithFlags(b->mark[1], c->stream, cudaEventRecordExternal);
     cudaError_t le = cudaGetLastError();
     e = cudaStreamEndCapture(c->stream, &g);
@@ -583,6 +588,8 @@ lpk_status lpk_batch_create(lpk_ctx *c, const lpk_work_unit *wu, int32_t n_units
     if (!st) st = batch_alloc(b, &p, sizeof(RoundDesc)), b->d_round = (RoundDesc *)p;
     if (!st) st = batch_alloc(b, &p, sizeof(AnchorRec) * (size_t)std::max<int64_t>(1, b->recs_cap)),
              b->d_recs = (AnchorRec *)p;
+    if (!st) st = batch_alloc(b, &p, sizeof(AnchorExt) * (size_t)std::max<int64_t>(1, b->recs_cap)),
+             b->d_exts = (AnchorExt *)p;
     if (!st) st = batch_alloc(b, &p, sizeof(unsigned long long)), b->d_counter = (unsigned long long *)p;
     if (!st) st = batch_alloc(b, &p, sizeof(DevWalk) * std::max<size_t>(1, b->walks.size())),
              b->d_walks = (DevWalk *)p;

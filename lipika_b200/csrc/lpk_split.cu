@@ -13,22 +13,26 @@ namespace {
 // One thread per (tile, transmitter).
 __global__ void __launch_bounds__(128)
 k_split_anchor(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__restrict__ active, int32_t n_active,
-               int64_t t0, int64_t n_tiles, int32_t tile_len, AnchorRec *__restrict__ recs) {
+               int64_t t0, int64_t n_tiles, int32_t tile_len, AnchorRec *__restrict__ recs,
+               AnchorExt *__restrict__ exts) {
     const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= n_tiles * n_active) return;
     const int64_t tile = id / n_active;
     const int k = (int)(id - tile * n_active);
     const int64_t gs = (t0 + tile) * tile_len;  // absolute sample indices of the tile
     AnchorRec r;
-    fit_anchor(b, txs[active[k]], gs, gs + tile_len - 1, false, r);
+    AnchorExt x;
+    fit_anchor(b, txs[active[k]], gs, gs + tile_len - 1, false, r, x);
     recs[id] = r;
+    if (r.n_nodes > 1) exts[id] = x;
 }
 
 // One block per tile.
-template <int TILE, int THREADS, int MINB, bool DBG>
+template <int TILE, int THREADS, int MINB, bool DBG, bool UNOCC>
 __global__ void __launch_bounds__(THREADS, MINB)
 k_band_split(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__restrict__ active, int32_t n_active,
-             int64_t t0, const AnchorRec *__restrict__ recs, float2 *__restrict__ out, double *dbg_phase,
+             int64_t t0, const AnchorRec *__restrict__ recs, const AnchorExt *__restrict__ exts,
+             float2 *__restrict__ out, double *dbg_phase,
              double *dbg_temit, double *dbg_delay) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     DevTx *stx = reinterpret_cast<DevTx *>(smem_raw);
@@ -37,18 +41,21 @@ k_band_split(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__re
     stage_tile(txs, active, n_active, recs + tile * n_active, stx, srec, true);
     __syncthreads();
     const int64_t first = (t0 + tile) * TILE - b.i0;  // chunk index of the tile's first sample
-    split_tile<TILE / THREADS, THREADS, DBG>(b, stx, srec, n_active, first, out, dbg_phase, dbg_temit, dbg_delay);
+    split_tile<TILE / THREADS, THREADS, DBG, UNOCC>(b, stx, srec, exts + tile * n_active, n_active, first, out,
+                                                    dbg_phase, dbg_temit, dbg_delay);
 }
 
 using SplitKernel = void (*)(const DevBand, const DevTx *, const int32_t *, int32_t, int64_t, const AnchorRec *,
-                             float2 *, double *, double *, double *);
+                             const AnchorExt *, float2 *, double *, double *, double *);
 
 struct SplitShape {
     int tile, threads, minb;
-    SplitKernel fast, dbg;
+    SplitKernel fast, fast_unocc, dbg;
 };
 
-#define LPK_SPLIT_ENTRY(I, T, N, M) {T, N, M, k_band_split<T, N, M, false>, k_band_split<T, N, M, true>},
+#define LPK_SPLIT_ENTRY(I, T, N, M)                                                                              \
+    {T, N, M, k_band_split<T, N, M, false, false>, k_band_split<T, N, M, false, true>,                           \
+     k_band_split<T, N, M, true, false>},
 const SplitShape kShapes[kSplitVariants] = {LPK_SPLIT_VARIANTS(LPK_SPLIT_ENTRY)};
 #undef LPK_SPLIT_ENTRY
 
@@ -65,7 +72,8 @@ bool split_variant_info(int v, int *tile, int *threads, int *minb) {
 }
 
 size_t split_recs_bytes(int variant, int64_t i0, int64_t n, int32_t n_active) {
-    return sizeof(AnchorRec) * (size_t)split_tiles(i0, n, kShapes[variant].tile) * (size_t)n_active;
+    return (sizeof(AnchorRec) + sizeof(AnchorExt)) * (size_t)split_tiles(i0, n, kShapes[variant].tile) *
+           (size_t)n_active;
 }
 
 cudaError_t launch_band_split(int variant, const DevBand &b, const DevTx *d_tx, const int32_t *d_active,
@@ -77,20 +85,21 @@ cudaError_t launch_band_split(int variant, const DevBand &b, const DevTx *d_tx, 
     const int64_t n_tiles = split_tiles(b.i0, b.n, sh.tile);
     const int64_t na = n_tiles * n_active;
     AnchorRec *recs = (AnchorRec *)d_recs;
+    AnchorExt *exts = (AnchorExt *)(recs + na);  // 16-byte aligned: sizeof(AnchorRec) is a multiple of 16
     if (na > 0) {
         k_split_anchor<<<(unsigned)((na + 127) / 128), 128, 0, s>>>(b, d_tx, d_active, n_active, t0, n_tiles, sh.tile,
-                                                                     recs);
+                                                                     recs, exts);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
     const size_t smem = (sizeof(DevTx) + sizeof(AnchorRec)) * (size_t)n_active;
-    SplitKernel kern = dbg_phase ? sh.dbg : sh.fast;
+    SplitKernel kern = dbg_phase ? sh.dbg : (b.unocc_words ? sh.fast_unocc : sh.fast);
     if (smem > 40 * 1024) {  // leaves room for the kernel's static shared arrays
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    kern<<<(unsigned)n_tiles, sh.threads, smem, s>>>(b, d_tx, d_active, n_active, t0, recs, d_out, dbg_phase,
-                                                     dbg_temit, dbg_delay);
+    kern<<<(unsigned)n_tiles, sh.threads, smem, s>>>(b, d_tx, d_active, n_active, t0, recs, exts, d_out,
+                                                     dbg_phase, dbg_temit, dbg_delay);
     return cudaGetLastError();
 }
 

@@ -58,12 +58,12 @@ enum : int32_t { kRecExact = 1, kRecNavVary = 2, kRecGateOff = 4, kRecCaWide = 8
 struct __align__(16) AnchorRec {
     double tu0, tu_hi;                // fit range; Δ origin tu0
     // An iterate's query crosses up to kSplitNodes grid nodes inside a tile
-    // (a tile up to 3 grid steps long): piece p >= 1 starts at node[p - 1]
-    // (absolute query time, kSplitInf when absent).
-    double node0[kSplitNodes], node1[kSplitNodes];
-    double p0[kSplitNodes + 1][3];    // first-iterate delay pieces (unrounded query)
-    double p1[kSplitNodes + 1][3];    // second-iterate delay pieces (unrounded query)
-    double k0, k1[kSplitNodes + 1];   // ∂delay/∂(query time): first iterate, second iterate per piece
+    // (a tile up to 3 grid steps long): piece p >= 1 starts at the p-th node
+    // (absolute query time, kSplitInf when absent). Pieces 0-1 live here,
+    // pieces 2-3 of a tile with n_nodes > 1 in its AnchorExt.
+    double node0, node1;              // first node of each iterate
+    double p0[2][3], p1[2][3];        // first- / second-iterate delay pieces 0-1 (unrounded query)
+    double k0, k1[2];                 // ∂delay/∂(query time): first iterate, second iterate per piece
     double tie;                       // guard on a rounding tie of the second query (s)
     double ulp_q;                     // ulp of the absolute query time
     double tau_if;                    // 2π (f_tx - f_lo)
@@ -73,9 +73,18 @@ struct __align__(16) AnchorRec {
     int32_t nav_pm;                   // nav sign of the tile (1 with nav off; unused with kRecNavVary)
     int64_t sym_raw0, sym_pos0;       // framed kinds: raw symbol count at the tile start and its frame slot
     double chip_fl0;                  // C/A: a whole chip count at or below the tile's first chip
-    int32_t chip_m0, pad;             // C/A: chip_fl0 mod 1023
+    int32_t chip_m0;                  // C/A: chip_fl0 mod 1023
+    int32_t n_nodes;                  // most grid nodes either iterate crosses in the tile
 };
 static_assert(sizeof(AnchorRec) % 16 == 0, "AnchorRec arrays must keep 16-byte alignment");
+
+// Pieces 2-3 of a tile whose iterates cross more than one grid node (low
+// sample rates): read from global memory by the multi-node pass only.
+struct __align__(16) AnchorExt {
+    double node0[2], node1[2];        // second and third nodes
+    double p0[2][3], p1[2][3];        // pieces 2-3
+    double k1[2];
+};
 
 // Lerp position at epoch-relative time t with the segment forced to `lo`
 // (linear extrapolation beyond it), without rounding epoch + t: de is
@@ -167,7 +176,7 @@ constexpr double kSplitInf = __builtin_huge_val();
 // exact_only: the tile takes the reference-exact path for every sample
 // (fan-out under the plain FP64 solver, or with an antenna).
 __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, int64_t gs, int64_t ge, bool exact_only,
-                                           AnchorRec &r) {
+                                           AnchorRec &r, AnchorExt &x) {
     const double tls = (double)gs / b.fs, tle = (double)ge / b.fs;
     const double tus = tls - (b.clock_offset + b.clock_y0 * tls) - kSplitMargin;
     const double tue = tle - (b.clock_offset + b.clock_y0 * tle) + kSplitMargin;
@@ -176,19 +185,21 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
     const double de = tx.traj_kind != 0 ? b.epoch - tx.t0 : 0.0;
     r.tu0 = tus;
     r.tu_hi = tue;
-    for (int i = 0; i < kSplitNodes; ++i) r.node0[i] = r.node1[i] = kSplitInf;
+    r.node0 = r.node1 = kSplitInf;
+    r.n_nodes = 0;
+    for (int i = 0; i < 2; ++i) x.node0[i] = x.node1[i] = kSplitInf;
     r.tau_if = kTau * (tx.carrier - b.lo);
     r.flags = 0;
     r.nav_pm = 1;
     r.k0 = 0.0;
-    for (int p = 0; p <= kSplitNodes; ++p) {
-        r.k1[p] = 0.0;
-        for (int i = 0; i < 3; ++i) r.p0[p][i] = r.p1[p][i] = 0.0;
+    for (int p = 0; p < 2; ++p) {
+        r.k1[p] = x.k1[p] = 0.0;
+        for (int i = 0; i < 3; ++i) r.p0[p][i] = r.p1[p][i] = x.p0[p][i] = x.p1[p][i] = 0.0;
     }
     int64_t lo0s = 0, lo0e = 0, lo1s = 0, lo1e = 0;
     bool exact = exact_only;
     r.chip_fl0 = 0.0;
-    r.chip_m0 = r.pad = 0;
+    r.chip_m0 = 0;
     if (exact) {
         r.amp0 = r.amp1 = 0.0f;
         r.guard = r.ulp_q = r.tie = 0.0;
@@ -206,10 +217,13 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
         lo1e = seg_unrounded(tx, tue - d0e, de, c4);
         exact = c1 || c2 || c3 || c4 || lo0e < lo0s || lo0e > lo0s + kSplitNodes || lo1e < lo1s ||
                 lo1e > lo1s + kSplitNodes;
-        for (int i = 0; i < kSplitNodes; ++i) {
-            if (lo0s + i < lo0e) r.node0[i] = tx.t0 + (double)(lo0s + i + 1) * tx.dt;
-            if (lo1s + i < lo1e) r.node1[i] = tx.t0 + (double)(lo1s + i + 1) * tx.dt;
+        if (lo0s < lo0e) r.node0 = tx.t0 + (double)(lo0s + 1) * tx.dt;
+        if (lo1s < lo1e) r.node1 = tx.t0 + (double)(lo1s + 1) * tx.dt;
+        for (int i = 0; i < 2; ++i) {
+            if (lo0s + 1 + i < lo0e) x.node0[i] = tx.t0 + (double)(lo0s + 2 + i) * tx.dt;
+            if (lo1s + 1 + i < lo1e) x.node1[i] = tx.t0 + (double)(lo1s + 2 + i) * tx.dt;
         }
+        r.n_nodes = (int32_t)(lo0e - lo0s > lo1e - lo1s ? lo0e - lo0s : lo1e - lo1s);
     }
     double rs = 1.0, re = 1.0, te_s = tus, te_e = tue;
     if (!exact) {
@@ -223,12 +237,12 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
                 v[i] = iterate_unrounded(tx, tu, tu - kEmissionLag, de, lo0s + p, ox, oy, oz, b.inv_c, nullptr,
                                          nullptr);
             }
-            quad3(v[0], v[1], v[2], h, r.p0[p]);
+            quad3(v[0], v[1], v[2], h, p < 2 ? r.p0[p] : x.p0[p - 2]);
         }
         for (int64_t p = 0; p <= lo1e - lo1s; ++p) {
             for (int i = 0; i < 3; ++i)
                 v[i] = solve_unrounded(tx, tus + i * h, de, lo1s + p, ox, oy, oz, b.inv_c, nullptr, nullptr);
-            quad3(v[0], v[1], v[2], h, r.p1[p]);
+            quad3(v[0], v[1], v[2], h, p < 2 ? r.p1[p] : x.p1[p - 2]);
         }
         // ∂delay/∂(query time) at the tile middle: the first iterate on its
         // natural segment, the second per piece
@@ -238,11 +252,12 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
         double d0m = iterate_unrounded(tx, mid, tq0, de, seg_unrounded(tx, tq0, de, cl), ox, oy, oz, b.inv_c,
                                        nullptr, &r.k0);
         for (int64_t p = 0; p <= lo1e - lo1s; ++p)
-            iterate_unrounded(tx, mid, mid - d0m, de, lo1s + p, ox, oy, oz, b.inv_c, nullptr, &r.k1[p]);
+            iterate_unrounded(tx, mid, mid - d0m, de, lo1s + p, ox, oy, oz, b.inv_c, nullptr,
+                              p < 2 ? &r.k1[p] : &x.k1[p - 2]);
         solve_unrounded(tx, tus, de, lo1s, ox, oy, oz, b.inv_c, nullptr, &rs);
         solve_unrounded(tx, tue, de, lo1e, ox, oy, oz, b.inv_c, nullptr, &re);
         te_s = tus - poly2(r.p1[0], 0.0);
-        te_e = tue - poly2(r.p1[lo1e - lo1s], 2.0 * h);
+        te_e = tue - poly2(lo1e - lo1s < 2 ? r.p1[lo1e - lo1s] : x.p1[lo1e - lo1s - 2], 2.0 * h);
     }
     float amp_s = (float)(tx.amp_factor / rs), amp_e = (float)(tx.amp_factor / re);
     if (!exact && b.has_antenna) {
@@ -427,8 +442,11 @@ __device__ __forceinline__ void split_baseband(const DevTx &tx, const AnchorRec 
 // the second query, or within the guard band of an index boundary, sets
 // its bit in `redo` and is left to the exact path; `fit` has the bits of
 // the samples inside the tile's fit range. DBG stores the diagnostics.
-template <int K, bool DBG, bool KINK, int S, int THREADS>
-__device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, double epoch, const SampleCtx *sc,
+// NK: grid nodes inside the tile (0: one piece per iterate; 1: two
+// pieces; kSplitNodes: up to four pieces, selected per sample).
+template <int K, bool DBG, int NK, int S, int THREADS>
+__device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, const AnchorExt *X, double epoch,
+                                           const SampleCtx *sc,
                                            unsigned fit, float *ar, float *ai, unsigned &redo, int64_t first,
                                            double *dbg_phase, double *dbg_temit, double *dbg_delay) {
     const double tu0 = R.tu0, k0 = R.k0, tie = R.tie;
@@ -444,10 +462,14 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
         const double tu = __dsub_rn(c.tl, c.dl);  // src/pipeline.rs:927
         const double d = tu - tu0;
         double t1s, poly1, k1;
-        if constexpr (KINK) {
+        if constexpr (NK > 0) {
             const double q = __dadd_rn(epoch, __dsub_rn(tu, kEmissionLag));
-            const int i0 = (q >= R.node0[0]) + (q >= R.node0[1]) + (q >= R.node0[2]);
+            const int i0 = q >= R.node0;
             const double *p0 = R.p0[i0];
+            if constexpr (NK > 1) {
+                const int j0 = (q >= X->node0[0]) + (q >= X->node0[1]);
+                if (j0 > 0) p0 = X->p0[j0 - 1];
+            }
             t1s = tu - fma(d, fma(d, p0[2], p0[1]), p0[0]);
         } else {
             t1s = tu - fma(d, fma(d, a2, a1), a0);
@@ -456,11 +478,19 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
         const double s1 = __dadd_rn(epoch, t1r);  // its second query
         const double e1 = __dsub_rn(s1, epoch);
         bool ok = fabs(fabs(e1 - t1r) - half) > tie;
-        if constexpr (KINK) {
-            const int i1 = (s1 >= R.node1[0]) + (s1 >= R.node1[1]) + (s1 >= R.node1[2]);
+        if constexpr (NK > 0) {
+            const int i1 = s1 >= R.node1;
             const double *p1 = R.p1[i1];
+            double kk = R.k1[i1];
+            if constexpr (NK > 1) {
+                const int j1 = (s1 >= X->node1[0]) + (s1 >= X->node1[1]);
+                if (j1 > 0) {
+                    p1 = X->p1[j1 - 1];
+                    kk = X->k1[j1 - 1];
+                }
+            }
             poly1 = fma(d, fma(d, p1[2], p1[1]), p1[0]);
-            k1 = R.k1[i1];
+            k1 = kk;
         } else {
             poly1 = fma(d, fma(d, b2, b1), b0);
             k1 = ka;
@@ -501,10 +531,15 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
 // with the tile's transmitters and anchor records staged in shared memory.
 // Samples outside [0, b.n) are skipped; the transmitters are summed in
 // active-list order and the epilogue (AWGN, receiver chain) is applied.
-template <int S, int THREADS, bool DBG>
-__device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, const AnchorRec *srec, int n_active,
-                                           int64_t first, float2 *__restrict__ out, double *dbg_phase,
-                                           double *dbg_temit, double *dbg_delay) {
+// UNOCC: report per-transmitter occlusion words (b.unocc_words; antenna
+// bands of the per-band path only).
+template <int S, int THREADS, bool DBG, bool UNOCC>
+// xrec: the tile's AnchorExt records in global memory (index k per
+// transmitter), read only for tiles that cross more than one grid node.
+__device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, const AnchorRec *srec,
+                                           const AnchorExt *xrec, int n_active, int64_t first,
+                                           float2 *__restrict__ out, double *dbg_phase, double *dbg_temit,
+                                           double *dbg_delay) {
     SampleCtx sc[S];
     float ar[S], ai[S];
     unsigned live = 0, fit = 0;
@@ -573,15 +608,19 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
         unsigned redo = gate_off ? (DBG ? live : outside) : live;
         if (!(R.flags & kRecExact) && !gate_off) {
             redo = 0;
-            const bool kink = R.node0[0] < kSplitInf || R.node1[0] < kSplitInf;  // uniform over the block
+            // grid nodes inside the tile, uniform over the block
+            const int nk = R.n_nodes > 1 ? kSplitNodes : (R.node0 < kSplitInf || R.node1 < kSplitInf ? 1 : 0);
 #define LPK_PASS(KIND)                                                                                           \
     do {                                                                                                         \
-        if (kink)                                                                                                \
-            split_pass<KIND, DBG, true, S, THREADS>(T, R, b.epoch, sc, fit & live, ar, ai, redo, first,        \
-                                                    dbg_phase, dbg_temit, dbg_delay);                            \
+        if (nk == 0)                                                                                             \
+            split_pass<KIND, DBG, 0, S, THREADS>(T, R, xrec + k, b.epoch, sc, fit & live, ar, ai, redo, first, dbg_phase, \
+                                                 dbg_temit, dbg_delay);                                          \
+        else if (nk == 1)                                                                                        \
+            split_pass<KIND, DBG, 1, S, THREADS>(T, R, xrec + k, b.epoch, sc, fit & live, ar, ai, redo, first, dbg_phase, \
+                                                 dbg_temit, dbg_delay);                                          \
         else                                                                                                     \
-            split_pass<KIND, DBG, false, S, THREADS>(T, R, b.epoch, sc, fit & live, ar, ai, redo, first,       \
-                                                     dbg_phase, dbg_temit, dbg_delay);                           \
+            split_pass<KIND, DBG, kSplitNodes, S, THREADS>(T, R, xrec + k, b.epoch, sc, fit & live, ar, ai, redo, first,  \
+                                                           dbg_phase, dbg_temit, dbg_delay);                     \
     } while (0)
             switch (pass_kind(T, R)) {
             case kPassCa: LPK_PASS(kPassCa); break;
@@ -593,8 +632,10 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
             }
 #undef LPK_PASS
             redo &= live;
-            if (b.unocc_words && __any_sync(0xffffffffu, (fit & live) != 0) && (threadIdx.x & 31) == 0)
-                atomicOr(b.unocc_words + k, 1u);  // the tile's gain is non-zero throughout
+            if constexpr (UNOCC) {  // the tile's gain is non-zero throughout its fitted span
+                if (__any_sync(0xffffffffu, (fit & live) != 0) && (threadIdx.x & 31) == 0)
+                    atomicOr(b.unocc_words + k, 1u);
+            }
         }
         if (redo == 0) continue;
 #pragma unroll
@@ -604,7 +645,11 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
             double ph = 0.0, te = 0.0, rg = 0.0;
             const bool on = contribution(T, b, sc[s].tl, __dsub_rn(sc[s].tl, sc[s].dl), sc[s].dl, b.rx[0], b.rx[1],
                                          b.rx[2], cr, ci, &ph, &te, &rg);
-            if (on && b.unocc_words && !gate_off) atomicOr(b.unocc_words + k, 1u);
+            if constexpr (UNOCC) {
+                if (on && !gate_off) atomicOr(b.unocc_words + k, 1u);
+            } else {
+                (void)on;
+            }
             if (!gate_off || ((outside >> s) & 1u)) {
                 ar[s] = __fadd_rn(ar[s], cr);
                 ai[s] = __fadd_rn(ai[s], ci);
