@@ -84,7 +84,7 @@ __device__ __forceinline__ int find_slot_recs(const RoundDesc &rd, int64_t g) {
 
 // Scan blocks of every walk of the round (grid-stride, one block per scan
 // block): totals always, in-block prefixes for [bA, bB].
-__global__ void __launch_bounds__(kWalkThreads)
+__global__ void __launch_bounds__(kWalkThreads, LPK_WALK_MINB)
 k_batch_walk(const DevWalk *__restrict__ walks, const RoundDesc *__restrict__ rd) {
     __shared__ double warp_tot[kWalkThreads / 32];
     __shared__ double stage[kWalkStageDoubles];
@@ -124,27 +124,33 @@ k_batch_carry(const DevWalk *__restrict__ walks, const RoundDesc *__restrict__ r
         walk_group_carries(dw.totals, dw.gsum, rw.g_known, rw.bA, rw.bB, g, g == gA, dw.carry, sh);
 }
 
-// Anchor fits of every (slot, tile, transmitter) of the round.
-__global__ void __launch_bounds__(128)
+// Anchor fits of every (slot, tile, transmitter) of the round, one per
+// thread; each block builds its run of records in shared memory and stores
+// it contiguously.
+__global__ void __launch_bounds__(kAnchorThreads, LPK_ANCHOR_MINB)
 k_batch_anchor(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ units,
                const DevTx *__restrict__ txs, const int32_t *__restrict__ act, const RoundDesc *__restrict__ rd,
                AnchorRec *__restrict__ recs, AnchorExt *__restrict__ exts) {
+    __shared__ __align__(16) AnchorRec srec[kAnchorThreads];
     const int64_t total = rd->total_recs;
     const int tile_len = rd->tile;
-    for (int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; id < total;
-         id += (int64_t)gridDim.x * blockDim.x) {
-        const int sl = find_slot_recs(*rd, id);
-        const RoundUnit &ru = rd->s[sl];
-        const BatchUnit bu = units[ru.unit];
-        const int64_t local = id - ru.rec_off;
-        const int64_t tile = local / bu.n_active;
-        const int k = (int)(local - tile * bu.n_active);
-        const int64_t gs = (ru.t0 + tile) * tile_len;
-        AnchorRec r;
-        AnchorExt x;
-        fit_anchor(bands[ru.unit], txs[act[bu.act_off + k]], gs, gs + tile_len - 1, bu.exact_only != 0, r, x);
-        recs[id] = r;
-        if (r.n_nodes > 1) exts[id] = x;
+    for (int64_t base = (int64_t)blockIdx.x * kAnchorThreads; base < total;
+         base += (int64_t)gridDim.x * kAnchorThreads) {
+        const int64_t id = base + threadIdx.x;
+        if (id < total) {
+            const int sl = find_slot_recs(*rd, id);
+            const RoundUnit &ru = rd->s[sl];
+            const BatchUnit bu = units[ru.unit];
+            const int64_t local = id - ru.rec_off;
+            const int64_t tile = local / bu.n_active;
+            const int k = (int)(local - tile * bu.n_active);
+            const int64_t gs = (ru.t0 + tile) * tile_len;
+            fit_anchor(bands[ru.unit], txs[act[bu.act_off + k]], gs, gs + tile_len - 1, bu.exact_only != 0,
+                       srec[threadIdx.x], exts + id);
+        }
+        __syncthreads();
+        store_recs(srec, recs + base, (int)(total - base < kAnchorThreads ? total - base : kAnchorThreads));
+        __syncthreads();  // srec is rewritten by the next run
     }
 }
 
@@ -386,7 +392,7 @@ lpk_status build_graph(lpk_batch *b, int p) {
     cudaMemcpyAsync(b->d_round, b->h_round[p], sizeof(RoundDesc), cudaMemcpyHostToDevice, c->stream);
     cudaEventRecord(b->fork, c->stream);
     cudaStreamWaitEvent(b->side, b->fork, 0);
-    k_batch_anchor<<<b->anchor_grid, 128, 0, b->side>>>(b->d_bands, b->d_units, c->d_tx, b->d_act, b->d_round,
+    k_batch_anchor<<<b->anchor_grid, kAnchorThreads, 0, b->side>>>(b->d_bands, b->d_units, c->d_tx, b->d_act, b->d_round,
                                                         b->d_recs, b->d_exts);
     cudaEventRecord(b->join, b->side);
     if (!b->walks.empty()) {

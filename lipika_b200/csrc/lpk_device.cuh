@@ -315,8 +315,10 @@ __device__ __forceinline__ float2 noise_pair(uint64_t seed, int64_t g) {
 
 // Increments σ·z_k of the receiver clock's white-FM walk at master indices
 // k = 4q .. 4q+3: one Philox block (counter q, tag "CLOK", keyed by the
-// clock seed) gives two Box–Muller pairs in f32. Counter-based, so any
-// chunking or GPU regenerates the same walk.
+// clock seed) gives two Box–Muller pairs in f32, with the angle uniform on
+// [-π, π) and the hardware approximations of log, sin and cos (absolute
+// error ~2^-21, far below what the walk's moments resolve). Counter-based,
+// so any chunking or GPU regenerates the same walk.
 __device__ __forceinline__ void walk_increments4(uint64_t seed, int64_t q, double sigma, double z[4]) {
     const uint4 x = philox4x32_10(make_uint4((uint32_t)(uint64_t)q, (uint32_t)((uint64_t)q >> 32), 0x434C4F4Bu, 0u),
                                   make_uint2((uint32_t)seed, (uint32_t)(seed >> 32)));
@@ -325,9 +327,9 @@ __device__ __forceinline__ void walk_increments4(uint64_t seed, int64_t q, doubl
     for (int p = 0; p < 2; ++p) {
         const float u1 = __fmul_rn(__fadd_rn((float)(ua[p] >> 8), 1.0f), 0x1.0p-24f);
         const float u2 = __fmul_rn((float)(ub[p] >> 8), 0x1.0p-24f);
-        const float r = sqrtf(__fmul_rn(-2.0f, logf(u1)));
+        const float r = sqrtf(__fmul_rn(-2.0f, __logf(u1)));
         float sn, cs;
-        sincosf(__fmul_rn(6.28318548f, u2), &sn, &cs);
+        __sincosf(__fadd_rn(__fmul_rn(6.28318548f, u2), -3.14159274f), &sn, &cs);
         z[2 * p] = __dmul_rn(sigma, (double)__fmul_rn(r, cs));
         z[2 * p + 1] = __dmul_rn(sigma, (double)__fmul_rn(r, sn));
     }

@@ -132,7 +132,7 @@ k_rx_chain(const DevBand b, float2 *__restrict__ iq) {
 // ---------------------------------------------------------------- clock walk
 // One block per scan block (lpk_walk.cuh): its total (totals != NULL), or
 // ε(k) = carry(b) ⊕ P_b(k) for the master indices [kA, kB] it holds.
-__global__ void __launch_bounds__(kWalkThreads)
+__global__ void __launch_bounds__(kWalkThreads, LPK_WALK_MINB)
 k_walk_block(uint64_t seed, double sigma, int64_t b0, double *__restrict__ totals,
              const double *__restrict__ carry, double *__restrict__ eps, int64_t kA, int64_t kB) {
     __shared__ double warp_tot[kWalkThreads / 32];

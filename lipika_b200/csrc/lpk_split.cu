@@ -10,21 +10,23 @@ namespace lpk {
 
 namespace {
 
-// One thread per (tile, transmitter).
-__global__ void __launch_bounds__(128)
+// One thread per (tile, transmitter); the block's records are built in
+// shared memory and stored contiguously.
+__global__ void __launch_bounds__(kAnchorThreads, LPK_ANCHOR_MINB)
 k_split_anchor(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__restrict__ active, int32_t n_active,
                int64_t t0, int64_t n_tiles, int32_t tile_len, AnchorRec *__restrict__ recs,
                AnchorExt *__restrict__ exts) {
-    const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= n_tiles * n_active) return;
-    const int64_t tile = id / n_active;
-    const int k = (int)(id - tile * n_active);
-    const int64_t gs = (t0 + tile) * tile_len;  // absolute sample indices of the tile
-    AnchorRec r;
-    AnchorExt x;
-    fit_anchor(b, txs[active[k]], gs, gs + tile_len - 1, false, r, x);
-    recs[id] = r;
-    if (r.n_nodes > 1) exts[id] = x;
+    __shared__ __align__(16) AnchorRec srec[kAnchorThreads];
+    const int64_t base = (int64_t)blockIdx.x * kAnchorThreads, total = n_tiles * n_active;
+    const int64_t id = base + threadIdx.x;
+    if (id < total) {
+        const int64_t tile = id / n_active;
+        const int k = (int)(id - tile * n_active);
+        const int64_t gs = (t0 + tile) * tile_len;  // absolute sample indices of the tile
+        fit_anchor(b, txs[active[k]], gs, gs + tile_len - 1, false, srec[threadIdx.x], exts + id);
+    }
+    __syncthreads();
+    store_recs(srec, recs + base, (int)(total - base < kAnchorThreads ? total - base : kAnchorThreads));
 }
 
 // One block per tile.
@@ -87,7 +89,7 @@ cudaError_t launch_band_split(int variant, const DevBand &b, const DevTx *d_tx, 
     AnchorRec *recs = (AnchorRec *)d_recs;
     AnchorExt *exts = (AnchorExt *)(recs + na);  // 16-byte aligned: sizeof(AnchorRec) is a multiple of 16
     if (na > 0) {
-        k_split_anchor<<<(unsigned)((na + 127) / 128), 128, 0, s>>>(b, d_tx, d_active, n_active, t0, n_tiles, sh.tile,
+        k_split_anchor<<<(unsigned)((na + kAnchorThreads - 1) / kAnchorThreads), kAnchorThreads, 0, s>>>(b, d_tx, d_active, n_active, t0, n_tiles, sh.tile,
                                                                      recs, exts);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;

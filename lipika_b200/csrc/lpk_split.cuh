@@ -41,6 +41,10 @@ constexpr int kSplitVariants = 6;
 constexpr int kSplitNodes = 3;  // grid nodes an iterate's query may cross inside one tile
 constexpr int kSplitMaxTile = 1024;
 constexpr int kSplitMinTile = 512;
+constexpr int kAnchorThreads = 128;  // anchor kernels: records staged in shared memory per block
+#ifndef LPK_ANCHOR_MINB
+#define LPK_ANCHOR_MINB 5  // anchor blocks per SM (96 registers)
+#endif
 // Tiles are aligned to absolute band-sample indices and fitted over a tu range
 // that depends only on the tile and the clock's deterministic trend, widened
 // by kSplitMargin; a sample whose tu falls outside takes the exact path. So
@@ -132,18 +136,13 @@ __device__ __forceinline__ double iterate_unrounded(const DevTx &tx, double tu, 
     return r * inv_c;
 }
 
-// Both unrounded iterates at tu; the first iterate uses its natural segment,
-// the second is forced to lo1 (lo1 < 0: its natural segment).
-__device__ __forceinline__ double solve_unrounded(const DevTx &tx, double tu, double de, int64_t lo1, double ox,
-                                                  double oy, double oz, double inv_c, double *d0_out,
-                                                  double *range) {
-    bool cl;
-    double t0 = tu - kEmissionLag;
-    double d0 = iterate_unrounded(tx, tu, t0, de, seg_unrounded(tx, t0, de, cl), ox, oy, oz, inv_c, nullptr, nullptr);
-    if (d0_out) *d0_out = d0;
-    double t1 = tu - d0;
-    if (lo1 < 0) lo1 = seg_unrounded(tx, t1, de, cl);
-    return iterate_unrounded(tx, tu, t1, de, lo1, ox, oy, oz, inv_c, range, nullptr);
+// Copy n records from shared to global memory in 16-byte words, coalesced
+// (every thread of the block takes part).
+__device__ __forceinline__ void store_recs(const AnchorRec *__restrict__ s, AnchorRec *__restrict__ g, int n) {
+    const int4 *src = reinterpret_cast<const int4 *>(s);
+    int4 *dst = reinterpret_cast<int4 *>(g);
+    const int words = n * (int)(sizeof(AnchorRec) / 16);
+    for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
 }
 
 // Newton form of the quadratic through (0, v0), (h, v1), (2h, v2).
@@ -174,90 +173,106 @@ constexpr double kSplitInf = __builtin_huge_val();
 // band b. Everything depends only on the tile's absolute position, the
 // transmitter and the clock's deterministic trend, never on chunking.
 // exact_only: the tile takes the reference-exact path for every sample
-// (fan-out under the plain FP64 solver, or with an antenna).
+// (fan-out under the plain FP64 solver). r: the record (the anchor kernels
+// build it in shared memory); x: the tile's extension record, written only
+// when an iterate crosses more than one grid node (n_nodes > 1).
+//
+// The fits need each iterate at three times tu_i = tus + i h. The first
+// iterate on its natural segment at those times (d0_i) serves its own fit,
+// the second iterate's query times tu_i - d0_i, ∂/∂t at the middle (k0) and
+// the nodes; the second iterate per piece at the three times serves its fit,
+// k1 (middle) and the ranges at the ends (amplitude). Six evaluations for a
+// tile inside one grid segment.
 __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, int64_t gs, int64_t ge, bool exact_only,
-                                           AnchorRec &r, AnchorExt &x) {
+                                           AnchorRec &r, AnchorExt *x) {
     const double tls = (double)gs / b.fs, tle = (double)ge / b.fs;
     const double tus = tls - (b.clock_offset + b.clock_y0 * tls) - kSplitMargin;
-    const double tue = tle - (b.clock_offset + b.clock_y0 * tle) + kSplitMargin;
+    const double h = 0.5 * ((tle - (b.clock_offset + b.clock_y0 * tle) + kSplitMargin) - tus);
+    const double tue = tus + 2.0 * h;  // the third fit time, exactly
     const double ox = b.rx[0], oy = b.rx[1], oz = b.rx[2];
-    const double h = 0.5 * (tue - tus);
     const double de = tx.traj_kind != 0 ? b.epoch - tx.t0 : 0.0;
     r.tu0 = tus;
     r.tu_hi = tue;
     r.node0 = r.node1 = kSplitInf;
     r.n_nodes = 0;
-    for (int i = 0; i < 2; ++i) x.node0[i] = x.node1[i] = kSplitInf;
     r.tau_if = kTau * (tx.carrier - b.lo);
     r.flags = 0;
     r.nav_pm = 1;
     r.k0 = 0.0;
     for (int p = 0; p < 2; ++p) {
-        r.k1[p] = x.k1[p] = 0.0;
-        for (int i = 0; i < 3; ++i) r.p0[p][i] = r.p1[p][i] = x.p0[p][i] = x.p1[p][i] = 0.0;
+        r.k1[p] = 0.0;
+        for (int i = 0; i < 3; ++i) r.p0[p][i] = r.p1[p][i] = 0.0;
     }
-    int64_t lo0s = 0, lo0e = 0, lo1s = 0, lo1e = 0;
-    bool exact = exact_only;
     r.chip_fl0 = 0.0;
     r.chip_m0 = 0;
-    if (exact) {
+    if (exact_only) {
         r.amp0 = r.amp1 = 0.0f;
         r.guard = r.ulp_q = r.tie = 0.0;
         r.sym_raw0 = r.sym_pos0 = 0;
         r.flags = kRecExact;
         return;
     }
-    if (tx.traj_kind != 0) {
-        bool c1, c2, c3, c4;
-        lo0s = seg_unrounded(tx, tus - kEmissionLag, de, c1);
-        lo0e = seg_unrounded(tx, tue - kEmissionLag, de, c2);
-        double d0s = iterate_unrounded(tx, tus, tus - kEmissionLag, de, lo0s, ox, oy, oz, b.inv_c, nullptr, nullptr);
-        double d0e = iterate_unrounded(tx, tue, tue - kEmissionLag, de, lo0e, ox, oy, oz, b.inv_c, nullptr, nullptr);
-        lo1s = seg_unrounded(tx, tus - d0s, de, c3);
-        lo1e = seg_unrounded(tx, tue - d0e, de, c4);
-        exact = c1 || c2 || c3 || c4 || lo0e < lo0s || lo0e > lo0s + kSplitNodes || lo1e < lo1s ||
-                lo1e > lo1s + kSplitNodes;
-        if (lo0s < lo0e) r.node0 = tx.t0 + (double)(lo0s + 1) * tx.dt;
-        if (lo1s < lo1e) r.node1 = tx.t0 + (double)(lo1s + 1) * tx.dt;
-        for (int i = 0; i < 2; ++i) {
-            if (lo0s + 1 + i < lo0e) x.node0[i] = tx.t0 + (double)(lo0s + 2 + i) * tx.dt;
-            if (lo1s + 1 + i < lo1e) x.node1[i] = tx.t0 + (double)(lo1s + 2 + i) * tx.dt;
+    const double tu[3] = {tus, tus + h, tue};
+    double d0[3];
+    int64_t l0[3] = {0, 0, 0}, l1[3] = {0, 0, 0};
+    bool exact = false;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        bool cl = false;
+        const double tq = tu[i] - kEmissionLag;
+        if (tx.traj_kind != 0) {
+            l0[i] = seg_unrounded(tx, tq, de, cl);
+            exact |= cl;
         }
-        r.n_nodes = (int32_t)(lo0e - lo0s > lo1e - lo1s ? lo0e - lo0s : lo1e - lo1s);
+        d0[i] = iterate_unrounded(tx, tu[i], tq, de, l0[i], ox, oy, oz, b.inv_c, nullptr, i == 1 ? &r.k0 : nullptr);
+        if (tx.traj_kind != 0) {
+            l1[i] = seg_unrounded(tx, tu[i] - d0[i], de, cl);
+            exact |= cl;
+        }
     }
-    double rs = 1.0, re = 1.0, te_s = tus, te_e = tue;
+    const int64_t n0 = l0[2] - l0[0], n1 = l1[2] - l1[0];
+    exact |= n0 < 0 || n0 > kSplitNodes || n1 < 0 || n1 > kSplitNodes;
+    if (tx.traj_kind != 0) {
+        if (n0 > 0) r.node0 = tx.t0 + (double)(l0[0] + 1) * tx.dt;
+        if (n1 > 0) r.node1 = tx.t0 + (double)(l1[0] + 1) * tx.dt;
+        r.n_nodes = (int32_t)(n0 > n1 ? n0 : n1);
+        if (r.n_nodes > 1) {
+            for (int i = 0; i < 2; ++i) {
+                x->node0[i] = l0[0] + 1 + i < l0[2] ? tx.t0 + (double)(l0[0] + 2 + i) * tx.dt : kSplitInf;
+                x->node1[i] = l1[0] + 1 + i < l1[2] ? tx.t0 + (double)(l1[0] + 2 + i) * tx.dt : kSplitInf;
+                x->k1[i] = 0.0;
+                for (int j = 0; j < 3; ++j) x->p0[i][j] = x->p1[i][j] = 0.0;
+            }
+        }
+    }
+    double rs = 1.0, re = 1.0, te_s = tus, te_e = tue, d1m = 0.0;
     if (!exact) {
         // Each piece fits the iterate with its segment forced (the lerp
         // extrapolated linearly), over the whole tile: smooth, so a
         // quadratic through three points holds it well below 1 ps.
         double v[3];
-        for (int64_t p = 0; p <= lo0e - lo0s; ++p) {
-            for (int i = 0; i < 3; ++i) {
-                double tu = tus + i * h;
-                v[i] = iterate_unrounded(tx, tu, tu - kEmissionLag, de, lo0s + p, ox, oy, oz, b.inv_c, nullptr,
-                                         nullptr);
-            }
-            quad3(v[0], v[1], v[2], h, p < 2 ? r.p0[p] : x.p0[p - 2]);
-        }
-        for (int64_t p = 0; p <= lo1e - lo1s; ++p) {
+        for (int64_t p = 0; p <= n0; ++p) {
+#pragma unroll
             for (int i = 0; i < 3; ++i)
-                v[i] = solve_unrounded(tx, tus + i * h, de, lo1s + p, ox, oy, oz, b.inv_c, nullptr, nullptr);
-            quad3(v[0], v[1], v[2], h, p < 2 ? r.p1[p] : x.p1[p - 2]);
+                v[i] = l0[0] + p == l0[i] ? d0[i]
+                                          : iterate_unrounded(tx, tu[i], tu[i] - kEmissionLag, de, l0[0] + p, ox, oy,
+                                                              oz, b.inv_c, nullptr, nullptr);
+            quad3(v[0], v[1], v[2], h, p < 2 ? r.p0[p] : x->p0[p - 2]);
         }
-        // ∂delay/∂(query time) at the tile middle: the first iterate on its
-        // natural segment, the second per piece
-        bool cl;
-        const double mid = tus + h;
-        const double tq0 = mid - kEmissionLag;
-        double d0m = iterate_unrounded(tx, mid, tq0, de, seg_unrounded(tx, tq0, de, cl), ox, oy, oz, b.inv_c,
-                                       nullptr, &r.k0);
-        for (int64_t p = 0; p <= lo1e - lo1s; ++p)
-            iterate_unrounded(tx, mid, mid - d0m, de, lo1s + p, ox, oy, oz, b.inv_c, nullptr,
-                              p < 2 ? &r.k1[p] : &x.k1[p - 2]);
-        solve_unrounded(tx, tus, de, lo1s, ox, oy, oz, b.inv_c, nullptr, &rs);
-        solve_unrounded(tx, tue, de, lo1e, ox, oy, oz, b.inv_c, nullptr, &re);
+        for (int64_t p = 0; p <= n1; ++p) {
+            double k1 = 0.0;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                double *range = (i == 0 && p == 0) ? &rs : ((i == 2 && p == n1) ? &re : nullptr);
+                v[i] = iterate_unrounded(tx, tu[i], tu[i] - d0[i], de, l1[0] + p, ox, oy, oz, b.inv_c, range,
+                                         i == 1 ? &k1 : nullptr);
+            }
+            if (l1[0] + p == l1[1]) d1m = v[1];  // the second iterate on its natural segment at the middle
+            if (p < 2) r.k1[p] = k1; else x->k1[p - 2] = k1;
+            quad3(v[0], v[1], v[2], h, p < 2 ? r.p1[p] : x->p1[p - 2]);
+        }
         te_s = tus - poly2(r.p1[0], 0.0);
-        te_e = tue - poly2(lo1e - lo1s < 2 ? r.p1[lo1e - lo1s] : x.p1[lo1e - lo1s - 2], 2.0 * h);
+        te_e = tue - poly2(n1 < 2 ? r.p1[n1] : x->p1[n1 - 2], 2.0 * h);
     }
     float amp_s = (float)(tx.amp_factor / rs), amp_e = (float)(tx.amp_factor / re);
     if (!exact && b.has_antenna) {
@@ -266,8 +281,7 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
         // whose elevation range (three points, 1e-3 deg margin) touches a
         // discontinuity of the pattern (0 deg, the cutoff) takes the exact
         // path, one entirely below the cutoff is silent.
-        const double tm = tus + h;
-        const double te_m = tm - solve_unrounded(tx, tm, de, -1, ox, oy, oz, b.inv_c, nullptr, nullptr);
+        const double te_m = tu[1] - d1m;
         const double el_s = antenna_elevation(tx, b.epoch + te_s, ox, oy, oz);
         const double el_m = antenna_elevation(tx, b.epoch + te_m, ox, oy, oz);
         const double el_e = antenna_elevation(tx, b.epoch + te_e, ox, oy, oz);

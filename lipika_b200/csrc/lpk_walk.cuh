@@ -19,6 +19,9 @@ namespace lpk {
 
 constexpr int64_t kWalkBlock = 4096;  // master samples per scan block
 constexpr int kWalkThreads = 256;
+#ifndef LPK_WALK_MINB
+#define LPK_WALK_MINB 4  // scan blocks per SM (64 registers)
+#endif
 constexpr int kWalkPer = (int)(kWalkBlock / kWalkThreads);  // 16
 constexpr int64_t kGroupBlocks = 1024;                      // scan blocks per carry group
 constexpr int kGroupThreads = (int)kGroupBlocks;
