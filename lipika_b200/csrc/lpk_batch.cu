@@ -109,8 +109,25 @@ k_batch_walk(const DevWalk *__restrict__ walks, const RoundDesc *__restrict__ rd
     }
 }
 
-// Carries of the round's blocks [bA, bB] of every walk: blockIdx.y is the
-// walk, blocks stride over its carry groups (lpk_walk.cuh).
+// Sums of the carry groups [g_known, bB / kGroupBlocks) of every walk (the
+// groups the round completes), one block per group: blockIdx.y is the walk.
+__global__ void __launch_bounds__(kGroupThreads)
+k_batch_gsum(const DevWalk *__restrict__ walks, const RoundDesc *__restrict__ rd) {
+    __shared__ double sh[33];
+    const int w = (int)blockIdx.y;
+    if (w >= rd->n_walks) return;
+    const RoundWalk rw = rd->w[w];
+    if (rw.bB < rw.bA) return;
+    const DevWalk dw = walks[w];
+    for (int64_t h = rw.g_known + blockIdx.x; h < rw.bB / kGroupBlocks; h += gridDim.x) {
+        const double v = walk_group_sum(dw.totals, h, sh);
+        if (threadIdx.x == 0) dw.gsum[h] = v;
+    }
+}
+
+// Carries of the round's blocks [bA, bB] of every walk (lpk_walk.cuh), after
+// k_batch_gsum has stored every group sum they need: blockIdx.y is the walk,
+// blocks stride over its carry groups.
 __global__ void __launch_bounds__(kGroupThreads)
 k_batch_carry(const DevWalk *__restrict__ walks, const RoundDesc *__restrict__ rd) {
     __shared__ double sh[65];
@@ -120,8 +137,9 @@ k_batch_carry(const DevWalk *__restrict__ walks, const RoundDesc *__restrict__ r
     if (rw.bB < rw.bA) return;
     const DevWalk dw = walks[w];
     const int64_t gA = rw.bA / kGroupBlocks, gB = rw.bB / kGroupBlocks;
+    const int64_t known = gB > rw.g_known ? gB : rw.g_known;
     for (int64_t g = gA + blockIdx.x; g <= gB; g += gridDim.x)
-        walk_group_carries(dw.totals, dw.gsum, rw.g_known, rw.bA, rw.bB, g, g == gA, dw.carry, sh);
+        walk_group_carries(dw.totals, dw.gsum, known, rw.bA, rw.bB, g, false, dw.carry, sh);
 }
 
 // Anchor fits of every (slot, tile, transmitter) of the round, one per
@@ -397,7 +415,8 @@ lpk_status build_graph(lpk_batch *b, int p) {
     cudaEventRecord(b->join, b->side);
     if (!b->walks.empty()) {
         k_batch_walk<<<b->walk_grid, kWalkThreads, 0, c->stream>>>(b->d_walks, b->d_round);
-        k_batch_carry<<<dim3(8, (unsigned)b->walks.size()), kGroupThreads, 0, c->stream>>>(b->d_walks, b->d_round);
+        k_batch_gsum<<<dim3(16, (unsigned)b->walks.size()), kGroupThreads, 0, c->stream>>>(b->d_walks, b->d_round);
+        k_batch_carry<<<dim3(16, (unsigned)b->walks.size()), kGroupThreads, 0, c->stream>>>(b->d_walks, b->d_round);
     }
     cudaStreamWaitEvent(c->stream, b->join, 0);
     cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), c->stream);
@@ -704,7 +723,7 @@ lpk_status lpk_batch_run(lpk_batch *b, int64_t round) {
     if (e == cudaSuccess) e = cudaGraphLaunch(b->graph[p], c->stream);
     if (e == cudaSuccess) e = cudaEventRecord(b->done[p], c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "batch graph launch");
-    c->launches += 2 + (b->walks.empty() ? 0 : 2);
+    c->launches += 2 + (b->walks.empty() ? 0 : 3);
     b->last_parity = p;
     b->parity ^= 1;
     b->last_round = round;

@@ -175,7 +175,7 @@ def test_batch_profiling_times_each_fanout_without_changing_bits(ctx):
     ctx.check(L.lpk_profile_read(ctx.h, C.byref(ms), C.byref(fan), C.byref(alln)))
     ctx.check(L.lpk_profile_enable(ctx.h, 0))
     assert fan.value == b.n_rounds  # one timed persistent fan-out per round
-    assert alln.value == 4 * b.n_rounds  # walk scan, carries, anchors, fan-out
+    assert alln.value == 5 * b.n_rounds  # walk scan, group sums, carries, anchors, fan-out
     assert ms.value > 0.0
     ref = N.Batch(ctx, units, round_s=0.25).render()
     for x, y in zip(got, ref):
