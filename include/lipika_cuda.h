@@ -133,6 +133,22 @@ typedef struct lpk_tx_desc {
  * the fan-out reads, src/pipeline.rs:297-342). Replaces any earlier upload. */
 lpk_status lpk_scene_upload(lpk_ctx *ctx, const lpk_tx_desc *tx, int32_t n_tx);
 
+/* Trajectory tables of circular Keplerian orbits built on the GPU: replaces
+ * PrecomputedTrajectory::sample over CircularKeplerian::position_ecef
+ * (src/geometry/precomputed.rs:47-70, src/geometry/kepler.rs:32-85) for a
+ * set of orbits sharing one grid. For each orbit, the ECEF positions at
+ * t0_unix + i dt_s (i < n_points) are written to grid_xyz (host memory) as
+ * n_orbits consecutive (3, n_points) axis-major blocks, the layout of
+ * lpk_tx_desc.grid_xyz. FP64 with the host's operation order; the per-orbit
+ * constants come from the host's libm and the per-point sines and cosines
+ * from the GPU's, so an entry may differ from a host-built table in its
+ * last bits (~1e-9 m). */
+typedef struct lpk_kepler_orbit {
+    double semi_major_axis_m, inclination_deg, raan_deg, true_anomaly_deg_at_epoch, epoch_unix;
+} lpk_kepler_orbit;
+lpk_status lpk_kepler_tables(lpk_ctx *ctx, const lpk_kepler_orbit *orbits, int32_t n_orbits, double t0_unix,
+                             double dt_s, int64_t n_points, double *grid_xyz);
+
 enum { LPK_CLOCK_HOST = 0, LPK_CLOCK_DETERMINISTIC = 1, LPK_CLOCK_DEVICE_WALK = 2 };
 enum { LPK_RX_STATIONARY = 0, LPK_RX_PER_SAMPLE = 1 };
 enum { LPK_POST_GAIN = 0, LPK_POST_NONLINEARITY = 1, LPK_POST_ADC = 2 };

@@ -136,9 +136,14 @@ typedef struct lpk_scene_cfg {
     int32_t n_transmitters;
     const lpk_transmitter_cfg *transmitters;
     int32_t n_receivers;
-    int32_t reserved;
+    int32_t flags;                      /* LPK_SCENE_* below */
     const lpk_receiver_cfg *receivers;
 } lpk_scene_cfg;
+
+/* lpk_scene_cfg.flags: LPK_SCENE_DEVICE_TABLES builds the trajectory tables
+ * of circular Keplerian transmitters on the GPU (lpk_kepler_tables) instead
+ * of the host (needs a context). */
+enum { LPK_SCENE_DEVICE_TABLES = 1 };
 
 #ifdef __cplusplus
 }

@@ -17,7 +17,7 @@ OUT = os.path.join(HERE, "liblipika_cuda.so")
 BUILD = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU = ["lpk_abi.cu", "lpk_kernels.cu", "lpk_split.cu", "lpk_batch.cu", "lpk_mlp.cu", "lpk_noalloc.cu"]
+CU = ["lpk_abi.cu", "lpk_kernels.cu", "lpk_split.cu", "lpk_batch.cu", "lpk_mlp.cu", "lpk_noalloc.cu", "lpk_traj.cu"]
 CPP = ["lpk_host.cpp"]
 
 

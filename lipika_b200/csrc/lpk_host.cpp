@@ -290,6 +290,7 @@ struct TxHost {
     std::vector<lpk_cf32> sym;
     std::vector<double> gate_on;
     double bandwidth_hz = 0.0;
+    bool grid_pending = false;  // grid sized, to be filled on the GPU
 };
 
 struct RxHost {
@@ -324,7 +325,9 @@ double tx_bandwidth(const lpk_transmitter_cfg &t) {  // config/mod.rs:191-193, :
 }
 
 // Transmitter::from_config + build_signal (src/pipeline.rs:141-253, :311-341).
-lpk_status build_tx(const lpk_transmitter_cfg &c, const lpk_scene_cfg &scene, TxHost &h) {
+// device_grid: a circular Keplerian grid is sized here and filled later by
+// lpk_kepler_tables (h.grid_pending).
+lpk_status build_tx(const lpk_transmitter_cfg &c, const lpk_scene_cfg &scene, TxHost &h, bool device_grid) {
     lpk_tx_desc &d = h.desc;
     memset(&d, 0, sizeof d);
     const double render = scene.epoch_unix;
@@ -338,7 +341,8 @@ lpk_status build_tx(const lpk_transmitter_cfg &c, const lpk_scene_cfg &scene, Tx
         int64_t n = (int64_t)std::ceil(total / kGridDt) + 1;
         if (!(n >= 2) || n > (int64_t)1 << 31) return host_fail(LPK_EINVAL, "trajectory grid size out of range");
         h.grid.resize(3 * (size_t)n);
-        for (int64_t i = 0; i < n; ++i) {
+        h.grid_pending = device_grid;
+        for (int64_t i = 0; i < n && !device_grid; ++i) {
             double p[3];
             kepler(c.trajectory, start + (double)i * kGridDt, p);
             h.grid[i] = p[0];
@@ -495,10 +499,41 @@ lpk_status lpk_scene_prepare(lpk_ctx *ctx, const lpk_scene_cfg *cfg, lpk_scene *
     std::unique_ptr<lpk_scene> s(new lpk_scene());
     s->ctx = ctx;
     s->cfg = *cfg;
+    if ((cfg->flags & ~LPK_SCENE_DEVICE_TABLES) != 0) return host_fail(LPK_EINVAL, "unknown scene flags");
+    const bool device_grid = (cfg->flags & LPK_SCENE_DEVICE_TABLES) != 0;
+    if (device_grid && !ctx) return host_fail(LPK_EINVAL, "LPK_SCENE_DEVICE_TABLES needs a context");
     s->tx.resize((size_t)cfg->n_transmitters);
     for (int32_t i = 0; i < cfg->n_transmitters; ++i) {
-        lpk_status st = build_tx(cfg->transmitters[i], *cfg, s->tx[i]);
+        lpk_status st = build_tx(cfg->transmitters[i], *cfg, s->tx[i], device_grid);
         if (st) return st;
+    }
+    if (device_grid) {  // every pending grid shares the scene's start, step and length
+        std::vector<lpk_kepler_orbit> orbits;
+        std::vector<int32_t> which;
+        int64_t n = 0;
+        double start = 0.0;
+        for (int32_t i = 0; i < cfg->n_transmitters; ++i) {
+            if (!s->tx[i].grid_pending) continue;
+            const lpk_trajectory_cfg &t = cfg->transmitters[i].trajectory;
+            orbits.push_back({t.semi_major_axis_m, t.inclination_deg, t.raan_deg, t.true_anomaly_deg_at_epoch,
+                              t.epoch_unix});
+            which.push_back(i);
+            n = s->tx[i].desc.grid_n;
+            start = s->tx[i].desc.grid_t0_unix;
+        }
+        if (!orbits.empty()) {
+            std::vector<double> all(orbits.size() * 3 * (size_t)n);
+            lpk_status st = lpk_kepler_tables(ctx, orbits.data(), (int32_t)orbits.size(), start, kGridDt, n,
+                                              all.data());
+            if (st) return st;
+            for (size_t j = 0; j < which.size(); ++j) {
+                TxHost &h = s->tx[which[j]];
+                const size_t len = 3 * (size_t)n;
+                std::copy(all.begin() + (ptrdiff_t)(j * len), all.begin() + (ptrdiff_t)((j + 1) * len),
+                          h.grid.begin());
+                h.grid_pending = false;
+            }
+        }
     }
     s->rx.resize((size_t)cfg->n_receivers);
     for (int32_t r = 0; r < cfg->n_receivers; ++r) {

@@ -96,6 +96,11 @@ class WorkUnit(C.Structure):
                 ("reserved", C.c_int32), ("n_samples", C.c_int64)]
 
 
+class KeplerOrbit(C.Structure):
+    _fields_ = [("semi_major_axis_m", C.c_double), ("inclination_deg", C.c_double), ("raan_deg", C.c_double),
+                ("true_anomaly_deg_at_epoch", C.c_double), ("epoch_unix", C.c_double)]
+
+
 SINK_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.POINTER(CF32), C.c_int64)
 UNIT_SINK_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.c_int32, C.POINTER(CF32), C.c_int64)
 
@@ -120,6 +125,8 @@ SIGNATURES = {
     "lpk_probe_fp64_peak": (C.c_int32, [_VP, _D]),
     "lpk_gate_stats": (C.c_int32, [_VP, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int32]),
     "lpk_scene_upload": (C.c_int32, [_VP, C.POINTER(TxDesc), C.c_int32]),
+    "lpk_kepler_tables": (C.c_int32, [_VP, C.POINTER(KeplerOrbit), C.c_int32, C.c_double, C.c_double, C.c_int64,
+                                      _D]),
     "lpk_band_chunk": (C.c_int32, [_VP, C.POINTER(BandDesc), _I32, C.c_int32, C.c_int64, C.c_int64, _D, _D, _CF, _U8]),
     "lpk_band_chunk_device": (C.c_int32, [_VP, C.POINTER(BandDesc), _I32, C.c_int32, C.c_int64, C.c_int64,
                                           _VP, _VP, _VP, _VP]),

@@ -100,10 +100,13 @@ class Prepared:
 
     def __init__(self, scene: cfgmod.Scene, ctx: Optional[N.Context] = None,
                  time_base: int = A.LPK_TIME_BASE_SCENE,
-                 default_signal_epoch_unix: float = DEFAULT_SIGNAL_EPOCH_UNIX):
+                 default_signal_epoch_unix: float = DEFAULT_SIGNAL_EPOCH_UNIX, device_tables: bool = False):
+        """device_tables: build the circular Keplerian trajectory tables on the
+        GPU (lpk_kepler_tables) instead of the host."""
         self.scene = scene
         self.ctx = ctx or N.Context(0)
         self.cs = cfgmod.to_c(scene, time_base, default_signal_epoch_unix)
+        self.cs.cfg.flags = A.LPK_SCENE_DEVICE_TABLES if device_tables else 0
         h = C.c_void_p()
         N.check(N.lib().lpk_scene_prepare(self.ctx.h, C.byref(self.cs.cfg), C.byref(h)), self.ctx.h)
         self.h = h

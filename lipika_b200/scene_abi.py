@@ -25,6 +25,8 @@ LPK_NAV_FULL = 2
 LPK_TIME_BASE_SCENE = 0
 LPK_TIME_BASE_ABSOLUTE = 1
 
+LPK_SCENE_DEVICE_TABLES = 1  # lpk_scene_cfg.flags
+
 
 class TrajectoryCfg(C.Structure):
     _fields_ = [
@@ -100,6 +102,6 @@ class SceneCfg(C.Structure):
         ("gps_utc_offset_s", C.c_double), ("default_signal_epoch_unix", C.c_double),
         ("time_base", C.c_int32), ("n_transmitters", C.c_int32),
         ("transmitters", C.POINTER(TransmitterCfg)),
-        ("n_receivers", C.c_int32), ("reserved", C.c_int32),
+        ("n_receivers", C.c_int32), ("flags", C.c_int32),
         ("receivers", C.POINTER(ReceiverCfg)),
     ]

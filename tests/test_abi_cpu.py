@@ -211,3 +211,13 @@ def test_config_parsing_defaults():
     c1 = scenes.config_c1(1.0)
     assert c1.transmitters[0].effective_bandwidth_hz() == 2 * 9600.0
     assert c1.transmitters[1].effective_bandwidth_hz() == 2 * 1_023_000.0
+
+
+def test_device_tables_flag_needs_a_context_and_known_flags():
+    sc = scenes.config_c1(duration_s=0.1)
+    cs = cfg.to_c(sc, A.LPK_TIME_BASE_SCENE, 0.0)
+    h = C.c_void_p()
+    cs.cfg.flags = A.LPK_SCENE_DEVICE_TABLES
+    assert N.lib().lpk_scene_prepare(None, C.byref(cs.cfg), C.byref(h)) == N.LPK_EINVAL and not h.value
+    cs.cfg.flags = 1 << 5
+    assert N.lib().lpk_scene_prepare(None, C.byref(cs.cfg), C.byref(h)) == N.LPK_EINVAL and not h.value
