@@ -396,6 +396,7 @@ void lpk_ctx_destroy(lpk_ctx *c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     free_scene(c);
+    if (c->batch_kit) lpk::batch_kit_destroy(c->batch_kit);
     for (auto &w : c->walks) {
         if (w.d_tot) cudaFree(w.d_tot);
         if (w.d_carry) cudaFree(w.d_carry);

@@ -288,6 +288,7 @@ struct lpk_batch {
     cudaGraphNode_t prof_node[2][2] = {};
     int parity = 0, last_parity = 0;
     int64_t last_round = -1;
+    bool kit_complete = false;                      // every stream, event and descriptor above exists
     std::vector<lpk_cf32 *> staging[2];             // pinned host copies (lpk_batch_render), in the
                                                     // context's pinned pool
 };
@@ -481,6 +482,22 @@ lpk_status configure(lpk_batch *b, int variant, int bps) {
 
 }  // namespace
 
+namespace lpk {
+void batch_kit_destroy(BatchKit *k) {
+    if (!k) return;
+    for (void *h : k->h_round)
+        if (h) cudaFreeHost(h);
+    for (int i = 0; i < 2; ++i)
+        for (cudaEvent_t ev : {k->done[i], k->copied[i], k->mark[i]})
+            if (ev) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : {k->fork, k->join})
+        if (ev) cudaEventDestroy(ev);
+    for (cudaStream_t st : {k->side, k->copy})
+        if (st) cudaStreamDestroy(st);
+    delete k;
+}
+}  // namespace lpk
+
 extern "C" {
 
 int32_t lpk_split_variant_count(void) { return kSplitVariants; }
@@ -512,15 +529,19 @@ void lpk_batch_destroy(lpk_batch *b) {
     if (b->copy) cudaStreamSynchronize(b->copy);
     drop_graphs(b);
     for (void *p : b->allocs) pool_free(b->ctx, p);
-    for (auto &h : b->h_round)
-        if (h) cudaFreeHost(h);
-    for (int i = 0; i < 2; ++i)
-        for (cudaEvent_t ev : {b->done[i], b->copied[i], b->mark[i]})
-            if (ev) cudaEventDestroy(ev);
-    for (cudaEvent_t ev : {b->fork, b->join})
-        if (ev) cudaEventDestroy(ev);
-    for (cudaStream_t st : {b->side, b->copy})
-        if (st) cudaStreamDestroy(st);
+    BatchKit *k = new BatchKit();
+    for (int i = 0; i < 2; ++i) {
+        k->h_round[i] = b->h_round[i];
+        k->done[i] = b->done[i];
+        k->copied[i] = b->copied[i];
+        k->mark[i] = b->mark[i];
+    }
+    k->fork = b->fork;
+    k->join = b->join;
+    k->side = b->side;
+    k->copy = b->copy;
+    if (b->ctx && !b->ctx->batch_kit && b->kit_complete) b->ctx->batch_kit = k;  // the next batch reuses it
+    else batch_kit_destroy(k);
     delete b;
 }
 
@@ -635,19 +656,36 @@ lpk_status lpk_batch_create(lpk_ctx *c, const lpk_work_unit *wu, int32_t n_units
         if (!st) st = batch_alloc(b, &p, sizeof(double) * (size_t)(total_blocks[w] / kGroupBlocks + 1)),
                  h_walks[w].gsum = (double *)p;
     }
-    for (int i = 0; i < 2 && !st; ++i) {
-        if (cudaHostAlloc((void **)&b->h_round[i], sizeof(RoundDesc), cudaHostAllocDefault) != cudaSuccess)
-            st = fail(c, LPK_ENOMEM, "pinned round descriptor allocation failed");
-        else if (cudaEventCreateWithFlags(&b->done[i], cudaEventDisableTiming) != cudaSuccess ||
-                 cudaEventCreateWithFlags(&b->copied[i], cudaEventDisableTiming) != cudaSuccess ||
-                 cudaEventCreate(&b->mark[i]) != cudaSuccess)
-            st = fail(c, LPK_ECUDA, "event creation failed");
+    if (!st && c->batch_kit) {  // streams, events and pinned descriptors of the last batch
+        BatchKit *k = c->batch_kit;
+        c->batch_kit = nullptr;
+        for (int i = 0; i < 2; ++i) {
+            b->h_round[i] = (RoundDesc *)k->h_round[i];
+            b->done[i] = k->done[i];
+            b->copied[i] = k->copied[i];
+            b->mark[i] = k->mark[i];
+        }
+        b->fork = k->fork;
+        b->join = k->join;
+        b->side = k->side;
+        b->copy = k->copy;
+        delete k;
+    } else {
+        for (int i = 0; i < 2 && !st; ++i) {
+            if (cudaHostAlloc((void **)&b->h_round[i], sizeof(RoundDesc), cudaHostAllocDefault) != cudaSuccess)
+                st = fail(c, LPK_ENOMEM, "pinned round descriptor allocation failed");
+            else if (cudaEventCreateWithFlags(&b->done[i], cudaEventDisableTiming) != cudaSuccess ||
+                     cudaEventCreateWithFlags(&b->copied[i], cudaEventDisableTiming) != cudaSuccess ||
+                     cudaEventCreate(&b->mark[i]) != cudaSuccess)
+                st = fail(c, LPK_ECUDA, "event creation failed");
+        }
+        if (!st && (cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+                    cudaStreamCreateWithFlags(&b->copy, cudaStreamNonBlocking) != cudaSuccess ||
+                    cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+                    cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess))
+            st = fail(c, LPK_ECUDA, "stream or event creation failed");
     }
-    if (!st && (cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
-                cudaStreamCreateWithFlags(&b->copy, cudaStreamNonBlocking) != cudaSuccess ||
-                cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
-                cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess))
-        st = fail(c, LPK_ECUDA, "stream or event creation failed");
+    if (!st) b->kit_complete = true;
     if (!st) {
         cudaError_t e = cudaMemcpyAsync(b->d_bands, h_bands.data(), sizeof(DevBand) * (size_t)n_units,
                                         cudaMemcpyHostToDevice, c->stream);

@@ -22,6 +22,18 @@ struct WalkState {
     int64_t cap = 0;       // blocks the arrays hold
     double *d_tot = nullptr, *d_carry = nullptr, *d_gsum = nullptr;
 };
+
+// Streams, events and pinned round descriptors of a batch (lpk_batch.cu).
+// A context keeps the set of the last batch that ended, so the next batch
+// skips creating them (pinned allocations and stream creation are slow
+// driver calls, and freeing pinned memory synchronises the device).
+struct BatchKit {
+    void *h_round[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr}, copied[2] = {nullptr, nullptr}, mark[2] = {nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaStream_t side = nullptr, copy = nullptr;
+};
+void batch_kit_destroy(BatchKit *k);
 }  // namespace lpk
 
 struct lpk_ctx {
@@ -52,6 +64,7 @@ struct lpk_ctx {
     // scenes and batches, so repeated renders reuse memory without a device
     // synchronisation per allocation
     cudaMemPool_t pool = nullptr;
+    lpk::BatchKit *batch_kit = nullptr;  // kept from the last batch (see BatchKit)
 };
 
 namespace lpk {
