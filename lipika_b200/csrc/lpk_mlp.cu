@@ -16,9 +16,11 @@
 // converged delay is reported (the surrogate is judged, never trusted).
 //
 // The network is trained on this GPU from delays the converged solver
-// itself produces, by the kernels below: forward, backward and the weight
-// gradients run on the tensor cores as BF16 mma.sync tiles with FP32
-// accumulation; Adam updates FP32 master weights. Rounding points (BF16:
+// itself produces, by the kernels below: training's forward, backward and
+// weight gradients run as BF16 mma.sync tiles with FP32 accumulation (16- to
+// 64-wide products inside one warp's registers); inference runs on the
+// 5th-generation tensor cores (tcgen05.mma, accumulator in TMEM, 128-row
+// tiles); Adam updates FP32 master weights. Rounding points (BF16:
 // inputs, W1, W2, the first hidden layer and the two pre-activation
 // gradients; everything else FP32) are restated in oracle/mlp_ref.py.
 #include <algorithm>
@@ -148,25 +150,6 @@ __device__ __forceinline__ void warp_forward(const MlpWeights &S, float2 xg, flo
 __device__ __forceinline__ float2 load_x2(const float *__restrict__ x, int64_t row, int64_t n, int tig) {
     if (row >= n) return make_float2(0.0f, 0.0f);
     return make_float2(x[row * kF + 2 * tig], x[row * kF + 2 * tig + 1]);
-}
-
-// y = MLP(x) for n rows of normalised features (4 warps x 16 rows a block).
-__global__ void __launch_bounds__(128) k_mlp_forward(const float *__restrict__ p, const float *__restrict__ x,
-                                                     int64_t n, float *__restrict__ y) {
-    __shared__ MlpWeights S;
-    stage_weights(p, S);
-    __syncthreads();
-    const int lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
-    const int64_t warps = (int64_t)gridDim.x * 4;
-    for (int64_t r0 = ((int64_t)blockIdx.x * 4 + (threadIdx.x >> 5)) * 16; r0 < n; r0 += warps * 16) {
-        WarpAct A;
-        float yy[2];
-        warp_forward(S, load_x2(x, r0 + g, n, tig), load_x2(x, r0 + g + 8, n, tig), A, yy);
-        if (tig == 0) {
-            if (r0 + g < n) y[r0 + g] = yy[0];
-            if (r0 + g + 8 < n) y[r0 + g + 8] = yy[1];
-        }
-    }
 }
 
 // Sum of v over the 16 rows a warp holds (rows g and g+8 of every group):
@@ -494,6 +477,226 @@ __global__ void k_mlp_normalize(float *__restrict__ x, float *__restrict__ y, in
     y[i] = (y[i] - norm[2 * kF]) / norm[2 * kF + 1];
 }
 
+// ---------------------------------------------------------------------------
+// Forward pass on the 5th-generation tensor cores (inference: lpk_mlp_forward
+// and the learned start of the converged solve). One CTA of 4 warps takes
+// tiles of 128 rows: the tile's inputs and hidden layer are staged in shared
+// memory in the no-swizzle K-major core-matrix layout that tcgen05.mma reads
+// (8 rows x 16 bytes per core matrix; next 8-row group +128 B, next 8
+// K-elements +rows*16 B), one thread issues the MMAs (M = 128, N = 64,
+// K = 16 per instruction, BF16 operands, FP32 accumulator in TMEM), commits
+// them to an mbarrier, and each warp reads its 32 rows of the accumulator
+// back with tcgen05.ld for the tanh epilogue. Rounding points are those of
+// the mma.sync kernels (BF16 x, W1, W2 and first hidden layer; FP32
+// accumulation and everything else), so the CPU restatement covers both;
+// only the FP32 summation order differs (bias added after the products).
+constexpr int kTcRows = 128;          // rows per tile = the MMA's M
+constexpr uint32_t kTcCols = 64;      // TMEM columns: one 128 x 64 FP32 accumulator, reused by both layers
+// kind::f16 instruction descriptor: FP32 accumulator (bits 4-5 = 1), BF16 A
+// (7-9 = 1) and B (10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at 24.
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kH >> 3) << 17) |
+                              ((uint32_t)(kTcRows >> 4) << 24);
+constexpr int kTcSpin = 1 << 20;      // mbarrier polls before a wait gives up
+
+struct __align__(1024) TcSmem {
+    __nv_bfloat16 a1[2][kTcRows][8];  // x tile, K padded to 16: column groups 0-7 and 8-15 (zero)
+    __nv_bfloat16 a2[kH / 8][kTcRows][8];  // first hidden layer, 8 column groups
+    __nv_bfloat16 b1[2][kH][8];       // W1 (out x in), K padded to 16
+    __nv_bfloat16 b2[kH / 8][kH][8];  // W2 (out x in)
+    float bias1[kH], bias2[kH], w3[kH];
+    float b3;
+    unsigned long long bar;
+    uint32_t tmem;
+};
+// At most 7 CTAs of 29 KB or more fit on an SM (228 KB), so their TMEM
+// demand (7 x 64 columns) stays within the SM's 512 and tcgen05.alloc never
+// waits on another CTA.
+static_assert(sizeof(TcSmem) >= 29 * 1024 && 7 * kTcCols <= 512, "TMEM residency bound");
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor (no swizzle, K-major): start address,
+// leading byte offset (next 8 K-elements), stride byte offset (next 8 rows),
+// all in 16-byte units; version 1 (bit 46); base offset, LBO mode and layout
+// type 0.
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(da), "l"(db), "r"(kTcIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t phase) {
+    for (int it = 0; it < kTcSpin; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// This warp's 32 accumulator rows (lane = row), 64 FP32 columns.
+__device__ __forceinline__ void tc_load_row(uint32_t taddr, float v[kH]) {
+#pragma unroll
+    for (int q = 0; q < kH / 16; ++q) {
+        uint32_t r[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15}, [%16];\n"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr + (uint32_t)(16 * q)));
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[16 * q + i] = __uint_as_float(r[i]);
+    }
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// y = MLP(x) for n rows of normalised features; err (may be NULL) gets 1 if
+// an MMA completion wait gave up (the outputs are then incomplete).
+__global__ void __launch_bounds__(128, 1) k_mlp_forward_tc(const float *__restrict__ p, const float *__restrict__ x,
+                                                           int64_t n, float *__restrict__ y, int *__restrict__ err) {
+    __shared__ TcSmem S;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    // weights in the core-matrix layout (W1's K padded with zeros), biases,
+    // and the zero half of the input tile
+    for (int i = tid; i < 2 * kH * 8; i += blockDim.x) {
+        const int g = i / (kH * 8), o = (i / 8) % kH, c = i % 8, k = 8 * g + c;
+        S.b1[g][o][c] = __float2bfloat16_rn(k < kF ? p[kOffW1 + o * kF + k] : 0.0f);
+    }
+    for (int i = tid; i < kH * kH; i += blockDim.x) {
+        const int o = i / kH, k = i % kH;
+        S.b2[k / 8][o][k % 8] = __float2bfloat16_rn(p[kOffW2 + i]);
+    }
+    for (int i = tid; i < kH; i += blockDim.x) {
+        S.bias1[i] = p[kOffB1 + i];
+        S.bias2[i] = p[kOffB2 + i];
+        S.w3[i] = p[kOffW3 + i];
+    }
+    for (int i = tid; i < kTcRows * 8; i += blockDim.x) S.a1[1][i / 8][i % 8] = __float2bfloat16_rn(0.0f);
+    if (tid == 0) {
+        S.b3 = p[kOffB3];
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&S.bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem)),
+                     "r"(kTcCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = S.tmem, bar = smem_u32(&S.bar);
+    const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);  // this warp's lane quarter
+    const uint64_t d_a1 = tc_desc(smem_u32(&S.a1[0][0][0]), kTcRows * 16, 128);
+    const uint64_t d_b1 = tc_desc(smem_u32(&S.b1[0][0][0]), kH * 16, 128);
+    uint32_t phase = 0;
+    bool ok = true;
+    const int64_t tiles = (n + kTcRows - 1) / kTcRows;
+    for (int64_t t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+        const int64_t row = t * kTcRows + tid;
+        // inputs of this thread's row, BF16, into column group 0 of the tile
+        {
+            float v[kF];
+#pragma unroll
+            for (int k = 0; k < kF; ++k) v[k] = row < n ? x[row * kF + k] : 0.0f;
+            uint4 pk;
+            pk.x = pack2(v[0], v[1]);
+            pk.y = pack2(v[2], v[3]);
+            pk.z = pack2(v[4], v[5]);
+            pk.w = pack2(v[6], v[7]);
+            *reinterpret_cast<uint4 *>(&S.a1[0][tid][0]) = pk;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> the MMA's reads
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            tc_mma(tmem, d_a1, d_b1, 0u);  // layer 1: one K = 16 step
+            tc_commit(bar);
+        }
+        ok = __syncthreads_and(tc_wait(bar, phase));
+        phase ^= 1u;
+        if (!ok) break;
+        tc_fence_after();
+        float h[kH];
+        tc_load_row(trow, h);
+#pragma unroll
+        for (int g = 0; g < kH / 8; ++g) {  // tanh, BF16, into the second layer's A tile
+            uint4 pk;
+            pk.x = pack2(tanhf(h[8 * g + 0] + S.bias1[8 * g + 0]), tanhf(h[8 * g + 1] + S.bias1[8 * g + 1]));
+            pk.y = pack2(tanhf(h[8 * g + 2] + S.bias1[8 * g + 2]), tanhf(h[8 * g + 3] + S.bias1[8 * g + 3]));
+            pk.z = pack2(tanhf(h[8 * g + 4] + S.bias1[8 * g + 4]), tanhf(h[8 * g + 5] + S.bias1[8 * g + 5]));
+            pk.w = pack2(tanhf(h[8 * g + 6] + S.bias1[8 * g + 6]), tanhf(h[8 * g + 7] + S.bias1[8 * g + 7]));
+            *reinterpret_cast<uint4 *>(&S.a2[g][tid][0]) = pk;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();  // every warp has read the layer-1 accumulator and written its rows
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int kk = 0; kk < kH / 16; ++kk)  // layer 2: four K = 16 steps
+                tc_mma(tmem, tc_desc(smem_u32(&S.a2[2 * kk][0][0]), kTcRows * 16, 128),
+                       tc_desc(smem_u32(&S.b2[2 * kk][0][0]), kH * 16, 128), kk > 0 ? 1u : 0u);
+            tc_commit(bar);
+        }
+        ok = __syncthreads_and(tc_wait(bar, phase));
+        phase ^= 1u;
+        if (!ok) break;
+        tc_fence_after();
+        tc_load_row(trow, h);
+        float s = 0.0f;
+#pragma unroll
+        for (int c = 0; c < kH; ++c) s = fmaf(tanhf(h[c] + S.bias2[c]), S.w3[c], s);
+        if (row < n) y[row] = s + S.b3;
+        tc_fence_before();
+        __syncthreads();  // the tiles and the accumulator are reused by the next tile
+        tc_fence_after();
+    }
+    if (!ok && tid == 0 && err) atomicOr(err, 1);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols) : "memory");
+    }
+}
+
+// The tensor-core forward over n rows on `st`; d_err: one int of device memory.
+cudaError_t launch_mlp_forward(const float *d_p, const float *d_x, int64_t n, float *d_y, int *d_err, int sms,
+                               cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(d_err, 0, sizeof(int), st);
+    if (e != cudaSuccess || n <= 0) return e;
+    const int64_t tiles = (n + kTcRows - 1) / kTcRows;
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, 4 * (int64_t)sms));
+    k_mlp_forward_tc<<<grid, 128, 0, st>>>(d_p, d_x, n, d_y, d_err);
+    return cudaGetLastError();
+}
+
 }  // namespace
 }  // namespace lpk
 
@@ -634,19 +837,22 @@ lpk_status lpk_mlp_forward(lpk_mlp *m, const float *x, int64_t n, float *y) {
     if (n == 0) return LPK_OK;
     cudaSetDevice(c->device);
     const size_t bx = sizeof(float) * (size_t)n * kF, by = sizeof(float) * (size_t)n;
-    lpk_status s = ensure_scratch(c, bx + by + 256);
+    const size_t oy = (bx + 255) / 256 * 256, oe = oy + (by + 255) / 256 * 256;
+    lpk_status s = ensure_scratch(c, oe + 256);
     if (s) return s;
-    float *d_x = (float *)c->d_scratch, *d_y = (float *)((char *)c->d_scratch + (bx + 255) / 256 * 256);
+    float *d_x = (float *)c->d_scratch, *d_y = (float *)((char *)c->d_scratch + oy);
+    int *d_err = (int *)((char *)c->d_scratch + oe);
     if ((s = upload(c, d_x, x, bx))) return s;
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 63) / 64, 8 * sms));
-    k_mlp_forward<<<grid, 128, 0, c->stream>>>(m->d_p, d_x, n, d_y);
+    cudaError_t e = launch_mlp_forward(m->d_p, d_x, n, d_y, d_err, sms, c->stream);
     c->launches += 1;
-    cudaError_t e = cudaGetLastError();
+    int herr = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(y, d_y, by, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    return e == cudaSuccess ? LPK_OK : cuda_fail(c, e, "mlp forward");
+    if (e != cudaSuccess) return cuda_fail(c, e, "mlp forward");
+    return herr ? fail(c, LPK_ETIMEDOUT, "mlp forward: a tensor-core completion wait gave up") : LPK_OK;
 }
 
 lpk_status lpk_mlp_loss_grad(lpk_mlp *m, const float *x, const float *t, int64_t n, double *loss, float *grad) {
@@ -787,21 +993,22 @@ lpk_status lpk_solve_converged(lpk_ctx *c, int32_t tx, const double *rx, double 
     const size_t b_t = al(sizeof(double) * (size_t)n), b_o = al(sizeof(double) * (size_t)n),
                  b_i = al(sizeof(int32_t) * (size_t)n), b_e = al(sizeof(float) * (size_t)n),
                  b_x = start == LPK_START_LEARNED ? al(sizeof(float) * (size_t)n * kF) : 0,
-                 b_p = start == LPK_START_LEARNED ? al(sizeof(float) * (size_t)n) : 0;
-    if ((s = ensure_scratch(c, b_t + b_o + b_i + b_e + b_x + b_p))) return s;
+                 b_p = start == LPK_START_LEARNED ? al(sizeof(float) * (size_t)n) : 0, b_r = al(sizeof(int));
+    if ((s = ensure_scratch(c, b_t + b_o + b_i + b_e + b_x + b_p + b_r))) return s;
     char *base = (char *)c->d_scratch;
     double *d_t = (double *)base, *d_o = (double *)(base + b_t);
     int32_t *d_i = (int32_t *)(base + b_t + b_o);
     float *d_e = (float *)(base + b_t + b_o + b_i), *d_x = (float *)(base + b_t + b_o + b_i + b_e);
     float *d_p = (float *)(base + b_t + b_o + b_i + b_e + b_x);
+    int *d_err = (int *)(base + b_t + b_o + b_i + b_e + b_x + b_p);
     if ((s = upload(c, d_t, t_rel_utc, sizeof(double) * (size_t)n))) return s;
     const unsigned grid = (unsigned)((n + 127) / 128);
     if (start == LPK_START_LEARNED) {
         k_solve_features<<<grid, 128, 0, c->stream>>>(c->d_tx, tx, rx[0], rx[1], rx[2], epoch, d_t, n, m->d_norm, d_x);
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-        k_mlp_forward<<<(unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 63) / 64, 8 * sms)), 128, 0,
-                        c->stream>>>(m->d_p, d_x, n, d_p);
+        cudaError_t fe = launch_mlp_forward(m->d_p, d_x, n, d_p, d_err, sms, c->stream);
+        if (fe != cudaSuccess) return cuda_fail(c, fe, "mlp forward");
         c->launches += 2;
     }
     k_solve_converged<<<grid, 128, 0, c->stream>>>(c->d_tx, tx, rx[0], rx[1], rx[2], epoch, d_t, n, tol_s, max_iter,
@@ -815,8 +1022,12 @@ lpk_status lpk_solve_converged(lpk_ctx *c, int32_t tx, const double *rx, double 
         e = cudaMemcpyAsync(iters, d_i, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess && start_err)
         e = cudaMemcpyAsync(start_err, d_e, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
+    int herr = 0;
+    if (e == cudaSuccess && start == LPK_START_LEARNED)
+        e = cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    return e == cudaSuccess ? LPK_OK : cuda_fail(c, e, "converged solve");
+    if (e != cudaSuccess) return cuda_fail(c, e, "converged solve");
+    return herr ? fail(c, LPK_ETIMEDOUT, "learned start: a tensor-core completion wait gave up") : LPK_OK;
 }
 
 lpk_status lpk_solve_features(lpk_ctx *c, int32_t tx, const double *rx, double epoch, const double *t_rel_utc,
