@@ -692,7 +692,8 @@ cudaError_t launch_mlp_forward(const float *d_p, const float *d_x, int64_t n, fl
     cudaError_t e = cudaMemsetAsync(d_err, 0, sizeof(int), st);
     if (e != cudaSuccess || n <= 0) return e;
     const int64_t tiles = (n + kTcRows - 1) / kTcRows;
-    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, 4 * (int64_t)sms));
+    // five CTAs per SM: what the kernel's 96 registers allow (and 5 x 64 TMEM columns fit)
+    const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(tiles, 5 * (int64_t)sms));
     k_mlp_forward_tc<<<grid, 128, 0, st>>>(d_p, d_x, n, d_y, d_err);
     return cudaGetLastError();
 }

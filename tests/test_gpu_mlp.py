@@ -58,6 +58,31 @@ def test_forward_matches_cpu_restatement(ctx):
     m.close()
 
 
+def test_forward_tile_edges_and_many_rows(ctx):
+    """The tensor-core forward takes 128-row tiles: partial tiles, single
+    rows and a 4M-row batch (checked on a sample of rows) all match the CPU
+    restatement."""
+    import time
+    m = N.Mlp(ctx, seed=7)
+    p = _params(3)
+    m.set_params(p)
+    rng = np.random.default_rng(4)
+    for n in (1, 127, 128, 129, 4096 + 17):
+        x = rng.normal(size=(n, M.N_F)).astype(np.float32)
+        yr, _ = M.forward(p, x)
+        assert np.max(np.abs(m.forward(x) - yr)) <= FORWARD_ATOL
+    x = rng.normal(size=(1 << 22, M.N_F)).astype(np.float32)
+    m.forward(x)
+    t = time.perf_counter()
+    y = m.forward(x)
+    dt = time.perf_counter() - t
+    pick = rng.choice(x.shape[0], 4096, replace=False)
+    yr, _ = M.forward(p, x[pick])
+    assert np.max(np.abs(y[pick] - yr)) <= FORWARD_ATOL
+    print(f"forward of {x.shape[0]} rows with host copies: {dt * 1e3:.2f} ms")
+    m.close()
+
+
 @pytest.mark.parametrize("n", [128, 1000, 20000])
 def test_gradient_matches_cpu_restatement(ctx, n):
     m = N.Mlp(ctx, seed=7)
