@@ -173,8 +173,10 @@ k_batch_anchor(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ 
 }
 
 // The persistent fan-out: blocks take tiles from the round's counter until
-// none is left. A block restages the band and its transmitters only when
-// the next tile belongs to another unit.
+// none is left, claiming the next tile while they work on the current one
+// (the claim's latency is hidden and the end-of-tile barrier publishes it).
+// A block restages the band and its transmitters only when the next tile
+// belongs to another unit.
 template <int TILE, int THREADS, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB)
 k_batch_fanout(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ units,
@@ -186,14 +188,15 @@ k_batch_fanout(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ 
     DevTx *stx = reinterpret_cast<DevTx *>(smem_raw + ((sizeof(DevBand) + 15) / 16) * 16);
     AnchorRec *srec = reinterpret_cast<AnchorRec *>(reinterpret_cast<unsigned char *>(stx) +
                                                     sizeof(DevTx) * (size_t)max_active);
-    __shared__ unsigned long long s_next;
+    __shared__ unsigned long long s_next[2];
     int cur = -1;
     const int64_t total = rd->total_tiles;
-    for (;;) {
-        if (threadIdx.x == 0) s_next = atomicAdd(counter, 1ull);
-        __syncthreads();
-        const int64_t g = (int64_t)s_next;
+    if (threadIdx.x == 0) s_next[0] = atomicAdd(counter, 1ull);
+    __syncthreads();
+    for (int it = 0;; it ^= 1) {
+        const int64_t g = (int64_t)s_next[it];
         if (g >= total) break;
+        if (threadIdx.x == 0) s_next[it ^ 1] = atomicAdd(counter, 1ull);  // read after the end-of-tile barrier
         const int sl = find_slot_tiles(*rd, g);
         const RoundUnit &ru = rd->s[sl];
         const BatchUnit bu = units[ru.unit];
