@@ -99,6 +99,33 @@ def test_batch_split_matches_single_band(ctx, variant):
     prep2.close()
 
 
+def test_batch_noise_only_and_empty_units(ctx):
+    """A band no transmitter falls in (noise and the receiver chain only)
+    and a unit of zero length ride along in a batch: the first matches the
+    single-band kernel, the second yields nothing, and neither disturbs the
+    other units."""
+    prep = P.Prepared(_uneven_scene(), ctx)
+    for solver in (N.LPK_SOLVER_REFERENCE, N.LPK_SOLVER_SPLIT):
+        units = _units(prep, solver)
+        d0, _, n0 = units[0]
+        quiet = type(d0).from_buffer_copy(d0)
+        quiet.noise_seed = d0.noise_seed + 1000
+        empty = type(units[1][0]).from_buffer_copy(units[1][0])
+        units = units + [(quiet, [], n0), (empty, units[1][1], 0)]
+        single = _single(ctx, units[:-1]) + [np.zeros(0, np.complex64)]
+        b = N.Batch(ctx, units, round_s=0.25)
+        got = b.render()
+        b.close()
+        for u, (x, y) in enumerate(zip(got, single)):
+            assert x.shape == y.shape, (solver, u)
+            if solver == N.LPK_SOLVER_REFERENCE or u >= len(units) - 2:
+                assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), (solver, u, _rel(x, y))
+            else:
+                assert _rel(x, y) <= SPLIT_RTOL, (solver, u, _rel(x, y))
+        assert got[-2].size == n0 and np.any(got[-2] != 0)  # noise only
+    prep.close()
+
+
 def test_batch_round_length_and_order_do_not_change_bits(ctx):
     prep = P.Prepared(_uneven_scene(), ctx)
     units = _units(prep, N.LPK_SOLVER_SPLIT)
