@@ -298,9 +298,11 @@ __device__ __forceinline__ float2 box_muller(uint32_t a, uint32_t b) {
     float u1 = __fmul_rn(__fadd_rn((float)(a >> 8), 1.0f), 0x1.0p-24f);
     float u2 = __fmul_rn((float)(b >> 8), 0x1.0p-24f);
     float rr = sqrtf(__fmul_rn(-2.0f, logf(u1)));
-    float ang = __fmul_rn(6.28318548f, u2);
+    // angle uniform on [-pi, pi), where the hardware sin/cos approximation
+    // holds its 2^-21.4 absolute error bound
+    float ang = __fsub_rn(__fmul_rn(6.28318548f, u2), 3.14159274f);
     float s, c;
-    sincosf(ang, &s, &c);
+    __sincosf(ang, &s, &c);
     return make_float2(__fmul_rn(rr, c), __fmul_rn(rr, s));
 }
 __device__ __forceinline__ uint4 noise_block(uint64_t seed, int64_t g) {

@@ -156,7 +156,7 @@ void orc_noise_pair(uint64_t seed, int64_t g, float *z_re, float *z_im) {
     float u1 = ((float)(x[h] >> 8) + 1.0f) * 0x1.0p-24f;
     float u2 = (float)(x[h + 1] >> 8) * 0x1.0p-24f;
     float rr = sqrtf(-2.0f * logf(u1));
-    float ang = 6.28318548f * u2;
+    float ang = 6.28318548f * u2 - 3.14159274f;  /* the device takes sin/cos on [-pi, pi) */
     *z_re = rr * cosf(ang);
     *z_im = rr * sinf(ang);
 }
