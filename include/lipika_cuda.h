@@ -247,6 +247,12 @@ lpk_status lpk_tx_contribution(lpk_ctx *ctx, const lpk_band_desc *band, int32_t 
 lpk_status lpk_clock_device_delta(lpk_ctx *ctx, const lpk_band_desc *band, int64_t i0, int64_t n,
                                   double *delta_out);
 
+/* The local sample times t = i / fs_hz (src/pipeline.rs:918: `i as f64 / fs`)
+ * for i in [i0, i0 + n) exactly as the split fan-out forms them on the
+ * device (a reciprocal, a product and one fma correction instead of a
+ * division), copied to host memory; they must equal the IEEE quotient. */
+lpk_status lpk_sample_times(lpk_ctx *ctx, double fs_hz, int64_t i0, int64_t n, double *t_out);
+
 /* AWGN-free rx chain alone on n samples in place (RxChain::apply_post_sum,
  * src/rx/mod.rs:142-146): the band's post ops on caller-supplied f32 IQ,
  * so ADC codes can be compared on identical inputs. Host memory. */

@@ -773,6 +773,22 @@ lpk_status lpk_tx_contribution(lpk_ctx *c, const lpk_band_desc *band, int32_t tx
     return LPK_OK;
 }
 
+lpk_status lpk_sample_times(lpk_ctx *c, double fs_hz, int64_t i0, int64_t n, double *t_out) {
+    if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
+    if (!(fs_hz > 0.0) || !std::isfinite(fs_hz)) return fail(c, LPK_EINVAL, "fs_hz must be positive and finite");
+    if (n < 0 || i0 < 0 || i0 > ((int64_t)1 << 53) - n) return fail(c, LPK_EINVAL, "bad sample range");
+    if (n == 0) return LPK_OK;
+    if (!t_out) return fail(c, LPK_EINVAL, "t_out is NULL");
+    cudaSetDevice(c->device);
+    lpk_status st = ensure_scratch(c, sizeof(double) * (size_t)n);
+    if (st) return st;
+    cudaError_t e = launch_sample_times(fs_hz, i0, n, (double *)c->d_scratch, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(t_out, c->d_scratch, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    return e == cudaSuccess ? LPK_OK : cuda_fail(c, e, "sample times");
+}
+
 lpk_status lpk_clock_device_delta(lpk_ctx *c, const lpk_band_desc *band, int64_t i0, int64_t n, double *out) {
     if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
     DevBand b;

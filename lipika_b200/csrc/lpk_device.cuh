@@ -291,6 +291,17 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
     return c;
 }
 
+// t_local = i / fs (src/pipeline.rs:918), correctly rounded, without a
+// division instruction sequence: with y = RN(1/fs), q = RN(i y) is within
+// an ulp of i / fs, the remainder r = i - q fs is exact in one fma, and
+// RN(q + r y) is the correctly rounded quotient (Markstein, IBM J. Res. Dev.
+// 34, 1990). y comes from __drcp_rn, once per tile.
+__device__ __forceinline__ double sample_time(double i, double fs, double rfs) {
+    const double q = __dmul_rn(i, rfs);
+    const double r = __fma_rn(-q, fs, i);
+    return __fma_rn(r, rfs, q);
+}
+
 // AWGN for (seed, global band-sample index): one Philox block per pair of
 // indices 2p, 2p+1 (words 0-1 for 2p, words 2-3 for 2p+1), Box–Muller in
 // f32. Counter-based, so chunking cannot change it.

@@ -86,6 +86,7 @@ cudaError_t launch_tx_contribution(const DevBand &b, const DevTx *d_tx, int32_t 
                                    double *d_phase, double *d_temit, double *d_range, cudaStream_t s);
 cudaError_t launch_rx_chain(const DevBand &b, float2 *d_iq, cudaStream_t s);
 cudaError_t launch_band_delta(const DevBand &b, double *d_out, cudaStream_t s);
+cudaError_t launch_sample_times(double fs, int64_t i0, int64_t n, double *d_out, cudaStream_t s);
 // Split-precision fan-out (anchor kernel + per-sample kernel) in launch
 // shape `variant`; d_recs holds split_recs_bytes(variant, i0, n, n_active)
 // bytes. The dbg arrays (single transmitter only, may be NULL) receive the

@@ -164,6 +164,13 @@ k_walk_carries(const double *__restrict__ tot, double *__restrict__ gsum, int64_
     walk_group_carries(tot, gsum, g_known, bA, bB, g, blockIdx.x == 0, carry, sh);
 }
 
+// The split fan-out's sample times for indices i0 .. i0 + n - 1.
+__global__ void __launch_bounds__(kBlock) k_sample_times(double fs, int64_t i0, int64_t n, double *__restrict__ out) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    out[j] = sample_time((double)(i0 + j), fs, __drcp_rn(fs));
+}
+
 __global__ void __launch_bounds__(kBlock) k_band_delta(const DevBand b, double *__restrict__ out) {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= b.n) return;
@@ -200,6 +207,12 @@ __global__ void __launch_bounds__(256) k_fp64_probe(double *out, int iters) {
 
 cudaError_t launch_fp64_probe(double *d_out, int blocks, int iters, cudaStream_t s) {
     k_fp64_probe<<<blocks, 256, 0, s>>>(d_out, iters);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sample_times(double fs, int64_t i0, int64_t n, double *d_out, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    k_sample_times<<<grid_for(n), kBlock, 0, s>>>(fs, i0, n, d_out);
     return cudaGetLastError();
 }
 

@@ -558,6 +558,7 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
     float ar[S], ai[S];
     unsigned live = 0, fit = 0;
     const double tu0 = n_active > 0 ? srec[0].tu0 : 0.0, tu_hi = n_active > 0 ? srec[0].tu_hi : 0.0;
+    const double rfs = __drcp_rn(b.fs);
     static_assert(S % 2 == 0, "samples are held in adjacent pairs");
 #pragma unroll
     for (int s = 0; s < S; ++s) {
@@ -568,7 +569,7 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
         const bool lv = j >= 0 && j < b.n;
         const int64_t jc = j < 0 ? 0 : (j >= b.n ? b.n - 1 : j);
         ar[s] = ai[s] = 0.0f;
-        const double tl = __ddiv_rn((double)(b.i0 + jc), b.fs);  // src/pipeline.rs:918
+        const double tl = sample_time((double)(b.i0 + jc), b.fs, rfs);  // src/pipeline.rs:918
         const double dl = band_delta(b, jc, tl);
         const double tu = __dsub_rn(tl, dl);                      // :927
         const double t0q = __dsub_rn(tu, kEmissionLag);

@@ -154,3 +154,20 @@ def test_split_with_antenna_matches_reference(ctx):
     assert err <= IQ_RTOL
     assert np.array_equal(ref[1], spl[1])
     prep.close()
+
+
+@pytest.mark.parametrize("fs", [2.048e6, 48e3, 4.096e6, 250e3, 8.184e6, 1e6 / 3, 44100.0, 2.5e6 + 0.1,
+                                12345.678, 61.44e6])
+def test_split_sample_times_are_the_ieee_quotient(ctx, fs):
+    """The split fan-out forms t = i / fs with a reciprocal and one fma
+    correction (Markstein); every value must be the correctly rounded
+    quotient the reference computes (src/pipeline.rs:918), checked against
+    numpy's IEEE division over whole bands and far index ranges."""
+    L = N.lib()
+    n = 1 << 22
+    for i0 in (0, n, 1 << 28, (1 << 31) - 17, 10 ** 12 + 3, (1 << 52) - n):
+        t = np.zeros(n)
+        ctx.check(L.lpk_sample_times(ctx.h, fs, i0, n, t.ctypes.data_as(N._D)))
+        ref = np.arange(i0, i0 + n, dtype=np.int64).astype(np.float64) / fs
+        bad = np.flatnonzero(t != ref)
+        assert bad.size == 0, (fs, i0, bad[:5], t[bad[:5]], ref[bad[:5]])
