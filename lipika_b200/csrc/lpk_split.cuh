@@ -463,8 +463,12 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
                                            const SampleCtx *sc,
                                            unsigned fit, float *ar, float *ai, unsigned &redo, int64_t first,
                                            double *dbg_phase, double *dbg_temit, double *dbg_delay) {
-    const double tu0 = R.tu0, k0 = R.k0, tie = R.tie;
-    const double half = 0.5 * R.ulp_q, tau_if = R.tau_if, nts = tx.neg_tau_src, guard = R.guard;
+    const double tu0 = R.tu0, k0 = R.k0;
+    // A rounding error never exceeds half an ulp, so "|(|err| - half)| > tie"
+    // (not within `tie` of a tie) is |err| < half - tie; half and tie are
+    // powers of two, so the difference is exact (tie < 0: always true).
+    const double hm = 0.5 * R.ulp_q - R.tie;
+    const double tau_if = R.tau_if, nts = tx.neg_tau_src, guard = R.guard;
     const float amp0 = R.amp0, amp1 = R.amp1;
     // one piece per iterate (no grid node inside the tile): coefficients in registers
     const double a0 = R.p0[0][0], a1 = R.p0[0][1], a2 = R.p0[0][2];
@@ -491,7 +495,7 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
         const double t1r = fma(-k0, c.q0, t1s);  // the reference's t1
         const double s1 = __dadd_rn(epoch, t1r);  // its second query
         const double e1 = __dsub_rn(s1, epoch);
-        bool ok = fabs(fabs(e1 - t1r) - half) > tie;
+        bool ok = fabs(e1 - t1r) < hm;
         if constexpr (NK > 0) {
             const int i1 = s1 >= R.node1;
             const double *p1 = R.p1[i1];
