@@ -280,12 +280,15 @@ def config_c2(duration_s: float = 30.0, seed: int = 2026, n_rx: int = 32, noise:
 
 
 def config_c4(duration_s: float = 60.0, seed: int = 2026, n_rx: int = 16, noise: bool = True,
-              lo_hz: float = 1575.42e6) -> cfg.Scene:
-    """64 transmitters (16 each CW / OOK 1 kbit/s / 16-QAM 10 ksym/s / C/A PRN 1-16)."""
+              lo_hz: float = 1575.42e6, n_tx: int = 64) -> cfg.Scene:
+    """n_tx transmitters (64 by default: 16 each CW / OOK 1 kbit/s / 16-QAM
+    10 ksym/s / C/A PRN 1-16; a quarter of n_tx of each kind, PRNs cycling
+    1-32)."""
+    assert n_tx % 4 == 0
     rng = np.random.default_rng(seed)
     txs = []
-    for k in range(64):
-        kind = ("cw", "ook", "qam16", "ca_code")[k // 16]
+    for k in range(n_tx):
+        kind = ("cw", "ook", "qam16", "ca_code")[k // (n_tx // 4)]
         a = float(rng.uniform(6_900_000.0, 26_600_000.0))
         inc = float(rng.uniform(0.0, 98.0))
         raan = float(rng.uniform(0.0, 360.0))
@@ -303,9 +306,9 @@ def config_c4(duration_s: float = 60.0, seed: int = 2026, n_rx: int = 16, noise:
                       "payload_seed": int(rng.integers(0, 2**31)), "sync_word": [0, 0, 0, 0, 1, 0, 1, 0]}
             carrier = lo_hz + off
         else:
-            params = {"prn": k - 47, "epoch_unix": EPOCH, "nav": "dummy", "nav_seed": 0}
+            params = {"prn": 1 + (k - 3 * n_tx // 4) % 32, "epoch_unix": EPOCH, "nav": "dummy", "nav_seed": 0}
             carrier = lo_hz
-        txs.append(cfg.Transmitter(name=f"tx{k:02d}_{kind}", carrier_hz=carrier, kind=kind, params=params,
+        txs.append(cfg.Transmitter(name=f"tx{k:02d}_{kind}" if n_tx <= 100 else f"tx{k:03d}_{kind}", carrier_hz=carrier, kind=kind, params=params,
                                    trajectory=_kepler(a, inc, raan, ta), tx_power_dbw=20.0))
     rxs = []
     for r in range(n_rx):

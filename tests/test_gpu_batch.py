@@ -126,6 +126,26 @@ def test_batch_noise_only_and_empty_units(ctx):
     prep.close()
 
 
+def test_batch_with_256_transmitters_in_a_band(ctx):
+    """The most in-band transmitters a band takes (256): their tables and
+    anchor records staged in ~156 KB of shared memory (one fan-out block per
+    SM). Batch, single-band split kernel and the FP64 kernel agree."""
+    sc = scenes.config_c4(duration_s=0.05, n_rx=1, n_tx=256, noise=False)
+    prep = P.Prepared(sc, ctx)
+    assert [len(prep.active(r, b)) for (r, b) in prep.work()] == [256]
+    units = _units(prep, N.LPK_SOLVER_SPLIT)
+    split = _single(ctx, units)
+    ref = _single(ctx, _units(prep, N.LPK_SOLVER_REFERENCE))
+    b = N.Batch(ctx, units, round_s=0.02)
+    got = b.render()
+    v, bps, mx = b.config()
+    b.close()
+    print(f"256 transmitters: {bps} fan-out block(s) per SM (of {mx})")
+    assert _rel(got[0], split[0]) <= SPLIT_RTOL
+    assert _rel(got[0], ref[0]) <= 1e-5
+    prep.close()
+
+
 def test_batch_round_length_and_order_do_not_change_bits(ctx):
     prep = P.Prepared(_uneven_scene(), ctx)
     units = _units(prep, N.LPK_SOLVER_SPLIT)
