@@ -54,7 +54,7 @@ def _args():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--duration", type=float, default=120.0, help="scene duration (s)")
     p.add_argument("--chunk", type=int, default=1 << 24, help="samples per fan-out launch (value leg)")
-    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--e2e-steps", type=int, default=6)
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="target CPU time of the baseline sample")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -418,15 +418,18 @@ def run_ours(a):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0 = time.perf_counter()
         e0.record(stream)
+        per_step = []
         for _ in range(a.e2e_steps):
+            ts = time.perf_counter()
             e2e_step()
+            per_step.append(round(1e3 * (time.perf_counter() - ts), 2))
         e1.record(stream)
         e1.synchronize()
         wall = time.perf_counter() - t0
         ems = max_over_ranks(max(e0.elapsed_time(e1), 1e3 * wall))
         e2e = {"value": total_txrx * a.e2e_steps * ws / (ems * 1e-3), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(BYTES_PER_BAND_SAMPLE * total_band),
-               "ms_per_step": ems / a.e2e_steps,
+               "ms_per_step": ems / a.e2e_steps, "host_ms_each_step": per_step,
                "path": f"lpk_scene_prepare (trajectory tables built on the GPU) + lpk_generate_scene (C ABI): "
                        f"batched rounds of {a.e2e_round_s} s, outputs double-buffered into pinned host memory on a "
                        "copy stream"}
