@@ -362,6 +362,9 @@ lpk_status lpk_ctx_create(lpk_ctx **out, int32_t device) {
     e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev_start);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev_stop);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (e == cudaSuccess) {
         cudaMemPoolProps props;
         memset(&props, 0, sizeof props);
@@ -415,6 +418,10 @@ void lpk_ctx_destroy(lpk_ctx *c) {
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
     if (c->ev_start) cudaEventDestroy(c->ev_start);
     if (c->ev_stop) cudaEventDestroy(c->ev_stop);
+    if (c->aux) cudaStreamSynchronize(c->aux);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->aux) cudaStreamDestroy(c->aux);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -569,6 +576,19 @@ lpk_status lpk_scene_upload(lpk_ctx *c, const lpk_tx_desc *tx, int32_t n_tx) {
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Split path of a chunk entry point: the anchor fits on the side stream
+// (after everything already queued on the context's stream, so the previous
+// chunk's fan-out has read its records), the walk on the main stream, then
+// the fan-out once both are done.
+static cudaError_t split_fork_anchor(lpk_ctx *c, const DevBand &b, const int32_t *d_active, int32_t n_active,
+                                     void *d_recs) {
+    cudaError_t e = cudaEventRecord(c->ev_fork, c->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->aux, c->ev_fork, 0);
+    if (e == cudaSuccess) e = launch_split_anchor(c->split_variant, b, c->d_tx, d_active, n_active, d_recs, c->aux);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev_join, c->aux);
+    return e;
+}
+
 lpk_status lpk_band_chunk_device(lpk_ctx *c, const lpk_band_desc *band, const int32_t *active,
                                  int32_t n_active, int64_t i0, int64_t n, const double *d_delta,
                                  const double *d_rxpos, lpk_cf32 *d_out, uint8_t *d_unocc) {
@@ -597,12 +617,15 @@ lpk_status lpk_band_chunk_device(lpk_ctx *c, const lpk_band_desc *band, const in
                                     c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_uw, 0, sizeof(uint32_t) * 256, c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "chunk setup");
+    if (split && (e = split_fork_anchor(c, b, d_active, n_active, (char *)c->d_scratch + off_recs)) != cudaSuccess)
+        return cuda_fail(c, e, "anchor fits");
     if (span && (st = prepare_walk(c, band, i0, n, b, (double *)((char *)c->d_scratch + off_eps), span))) return st;
+    if (split && (e = cudaStreamWaitEvent(c->stream, c->ev_join, 0)) != cudaSuccess) return cuda_fail(c, e, "join");
     prof_begin(c);
     if (split) {
         b.unocc_words = b.has_antenna ? d_uw : nullptr;
-        e = launch_band_split(c->split_variant, b, c->d_tx, d_active, n_active, (char *)c->d_scratch + off_recs,
-                              (float2 *)d_out, nullptr, nullptr, nullptr, c->stream);
+        e = launch_split_fanout(c->split_variant, b, c->d_tx, d_active, n_active, (char *)c->d_scratch + off_recs,
+                                (float2 *)d_out, nullptr, nullptr, nullptr, c->stream);
     }
     else
         e = launch_band_reference(b, c->d_tx, d_active, n_active, (float2 *)d_out, d_uw, c->stream);
@@ -665,12 +688,15 @@ lpk_status lpk_band_chunk(lpk_ctx *c, const lpk_band_desc *band, const int32_t *
     if (e != cudaSuccess) return cuda_fail(c, e, "chunk upload");
     b.delta = d_delta;
     b.rxpos = d_rx;
+    if (split && (e = split_fork_anchor(c, b, d_active, n_active, base + off_recs)) != cudaSuccess)
+        return cuda_fail(c, e, "anchor fits");
     if (span && (st = prepare_walk(c, band, i0, n, b, (double *)(base + off_eps), span))) return st;
+    if (split && (e = cudaStreamWaitEvent(c->stream, c->ev_join, 0)) != cudaSuccess) return cuda_fail(c, e, "join");
     prof_begin(c);
     if (split) {
         b.unocc_words = b.has_antenna ? d_uw : nullptr;
-        e = launch_band_split(c->split_variant, b, c->d_tx, d_active, n_active, base + off_recs, d_out, nullptr,
-                              nullptr, nullptr, c->stream);
+        e = launch_split_fanout(c->split_variant, b, c->d_tx, d_active, n_active, base + off_recs, d_out, nullptr,
+                                nullptr, nullptr, c->stream);
     }
     else
         e = launch_band_reference(b, c->d_tx, d_active, n_active, d_out, d_uw, c->stream);

@@ -41,6 +41,10 @@ struct lpk_ctx {
     std::vector<lpk::WalkState> walks;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    // side stream of the chunk entry points: the split path's anchor fits
+    // run there, beside the clock walk on `stream`
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string err;
     // scene arena: every table of the uploaded transmitters
     std::vector<void *> scene_allocs;
@@ -93,6 +97,13 @@ cudaError_t launch_sample_times(double fs, int64_t i0, int64_t n, double *d_out,
 // reduced phase, emission time and delay.
 bool split_variant_info(int variant, int *tile, int *threads, int *min_blocks);
 size_t split_recs_bytes(int variant, int64_t i0, int64_t n, int32_t n_active);
+// The two halves of launch_band_split: the anchor fits (into d_recs) and
+// the fan-out that reads them.
+cudaError_t launch_split_anchor(int variant, const DevBand &b, const DevTx *d_tx, const int32_t *d_active,
+                               int32_t n_active, void *d_recs, cudaStream_t s);
+cudaError_t launch_split_fanout(int variant, const DevBand &b, const DevTx *d_tx, const int32_t *d_active,
+                                int32_t n_active, void *d_recs, float2 *d_out, double *dbg_phase, double *dbg_temit,
+                                double *dbg_delay, cudaStream_t s);
 cudaError_t launch_band_split(int variant, const DevBand &b, const DevTx *d_tx, const int32_t *d_active,
                               int32_t n_active, void *d_recs, float2 *d_out, double *dbg_phase, double *dbg_temit,
                               double *dbg_delay, cudaStream_t s);

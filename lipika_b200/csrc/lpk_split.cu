@@ -78,22 +78,31 @@ size_t split_recs_bytes(int variant, int64_t i0, int64_t n, int32_t n_active) {
            (size_t)n_active;
 }
 
-cudaError_t launch_band_split(int variant, const DevBand &b, const DevTx *d_tx, const int32_t *d_active,
-                              int32_t n_active, void *d_recs, float2 *d_out, double *dbg_phase, double *dbg_temit,
-                              double *dbg_delay, cudaStream_t s) {
+cudaError_t launch_split_anchor(int variant, const DevBand &b, const DevTx *d_tx, const int32_t *d_active,
+                               int32_t n_active, void *d_recs, cudaStream_t s) {
+    if (b.n <= 0) return cudaSuccess;
+    const SplitShape &sh = kShapes[variant];
+    const int64_t t0 = b.i0 / sh.tile;
+    const int64_t n_tiles = split_tiles(b.i0, b.n, sh.tile);
+    const int64_t na = n_tiles * n_active;
+    if (na <= 0) return cudaSuccess;
+    AnchorRec *recs = (AnchorRec *)d_recs;
+    AnchorExt *exts = (AnchorExt *)(recs + na);  // 16-byte aligned: sizeof(AnchorRec) is a multiple of 16
+    k_split_anchor<<<(unsigned)((na + kAnchorThreads - 1) / kAnchorThreads), kAnchorThreads, 0, s>>>(
+        b, d_tx, d_active, n_active, t0, n_tiles, sh.tile, recs, exts);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_split_fanout(int variant, const DevBand &b, const DevTx *d_tx, const int32_t *d_active,
+                                int32_t n_active, void *d_recs, float2 *d_out, double *dbg_phase, double *dbg_temit,
+                                double *dbg_delay, cudaStream_t s) {
     if (b.n <= 0) return cudaSuccess;
     const SplitShape &sh = kShapes[variant];
     const int64_t t0 = b.i0 / sh.tile;
     const int64_t n_tiles = split_tiles(b.i0, b.n, sh.tile);
     const int64_t na = n_tiles * n_active;
     AnchorRec *recs = (AnchorRec *)d_recs;
-    AnchorExt *exts = (AnchorExt *)(recs + na);  // 16-byte aligned: sizeof(AnchorRec) is a multiple of 16
-    if (na > 0) {
-        k_split_anchor<<<(unsigned)((na + kAnchorThreads - 1) / kAnchorThreads), kAnchorThreads, 0, s>>>(b, d_tx, d_active, n_active, t0, n_tiles, sh.tile,
-                                                                     recs, exts);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-    }
+    AnchorExt *exts = (AnchorExt *)(recs + na);
     const size_t smem = (sizeof(DevTx) + sizeof(AnchorRec)) * (size_t)n_active;
     SplitKernel kern = dbg_phase ? sh.dbg : (b.unocc_words ? sh.fast_unocc : sh.fast);
     if (smem > 40 * 1024) {  // leaves room for the kernel's static shared arrays
@@ -103,6 +112,15 @@ cudaError_t launch_band_split(int variant, const DevBand &b, const DevTx *d_tx, 
     kern<<<(unsigned)n_tiles, sh.threads, smem, s>>>(b, d_tx, d_active, n_active, t0, recs, exts, d_out,
                                                      dbg_phase, dbg_temit, dbg_delay);
     return cudaGetLastError();
+}
+
+cudaError_t launch_band_split(int variant, const DevBand &b, const DevTx *d_tx, const int32_t *d_active,
+                              int32_t n_active, void *d_recs, float2 *d_out, double *dbg_phase, double *dbg_temit,
+                              double *dbg_delay, cudaStream_t s) {
+    cudaError_t e = launch_split_anchor(variant, b, d_tx, d_active, n_active, d_recs, s);
+    if (e != cudaSuccess) return e;
+    return launch_split_fanout(variant, b, d_tx, d_active, n_active, d_recs, d_out, dbg_phase, dbg_temit, dbg_delay,
+                               s);
 }
 
 }  // namespace lpk
