@@ -465,6 +465,14 @@ enum { LPK_GEN_AUTOTUNE = 8 };
 lpk_status lpk_generate_scene(lpk_scene *s, uint64_t seed_base, double round_s, int32_t flags,
                               lpk_unit_sink_fn sink, void *user);
 
+/* run_scene_to_dir (src/pipeline.rs:494-536) through lpk_generate_scene:
+ * work unit w's samples are appended to paths[w] (raw little-endian
+ * complex64, StreamingC64Writer, src/output/mod.rs:100-147) from the pinned
+ * staging while the next round renders. The JSON sidecars are written by
+ * the caller, which holds the band metadata. */
+lpk_status lpk_generate_scene_to_files(lpk_scene *s, uint64_t seed_base, double round_s, int32_t flags,
+                                       const char *const *paths);
+
 /* Host clock stream (ClockStream, src/clock/mod.rs:229-347) exposed for
  * tests: delta_t_at over n monotone times. */
 typedef struct lpk_clock lpk_clock;

@@ -816,4 +816,29 @@ lpk_status lpk_generate_band_to_file(lpk_scene *s, int32_t r, int32_t b, uint64_
     return st;
 }
 
+lpk_status lpk_generate_scene_to_files(lpk_scene *s, uint64_t seed_base, double round_s, int32_t flags,
+                                       const char *const *paths) {
+    if (!s || !paths) return host_fail(LPK_EINVAL, "NULL scene or paths");
+    const int32_t n_work = (int32_t)s->work.size();
+    std::vector<FILE *> files((size_t)n_work, nullptr);
+    lpk_status st = LPK_OK;
+    for (int32_t w = 0; w < n_work && !st; ++w) {
+        if (!paths[w]) st = host_fail(LPK_EINVAL, "a work unit's path is NULL");
+        else if (!(files[w] = fopen(paths[w], "wb")))
+            st = host_fail(LPK_EINVAL, std::string("cannot create ") + paths[w] + ": " + strerror(errno));
+    }
+    if (!st) {
+        // each chunk is appended from the pinned staging on this thread while
+        // the GPU renders the next round
+        auto sink = [](void *user, int32_t w, const lpk_cf32 *chunk, int64_t n) -> int32_t {
+            FileSink fs{((FILE **)user)[w]};
+            return file_sink(&fs, chunk, n);
+        };
+        st = lpk_generate_scene(s, seed_base, round_s, flags, sink, files.data());
+    }
+    for (FILE *f : files)
+        if (f && fclose(f) != 0 && !st) st = host_fail(LPK_EINVAL, "closing an IQ file failed");
+    return st;
+}
+
 }  // extern "C"

@@ -125,6 +125,8 @@ SIGNATURES = {
     "lpk_probe_fp64_peak": (C.c_int32, [_VP, _D]),
     "lpk_gate_stats": (C.c_int32, [_VP, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int32]),
     "lpk_scene_upload": (C.c_int32, [_VP, C.POINTER(TxDesc), C.c_int32]),
+    "lpk_generate_scene_to_files": (C.c_int32, [_VP, C.c_uint64, C.c_double, C.c_int32,
+                                                 C.POINTER(C.c_char_p)]),
     "lpk_sample_times": (C.c_int32, [_VP, C.c_double, C.c_int64, C.c_int64, _D]),
     "lpk_kepler_tables": (C.c_int32, [_VP, C.POINTER(KeplerOrbit), C.c_int32, C.c_double, C.c_double, C.c_int64,
                                       _D]),

@@ -231,13 +231,33 @@ def run_scene(scene: cfgmod.Scene, rng_seed_base: int, ctx: Optional[N.Context] 
 
 def run_scene_to_dir(scene: cfgmod.Scene, rng_seed_base: int, directory: str,
                      chunk_samples: int = DEFAULT_CHUNK_SAMPLES, n_threads: int = 0,
-                     ctx: Optional[N.Context] = None, noise: bool = True) -> list[OutputManifest]:
+                     ctx: Optional[N.Context] = None, noise: bool = True, device_clock: bool = False,
+                     round_s: float = 4.0) -> list[OutputManifest]:
     """Stream each band to <dir>/<rx>__<band>.iq.c64 + .iq.json (src/pipeline.rs:494-536).
 
-    `n_threads` is accepted for signature parity; the fan-out runs on the GPU."""
+    `n_threads` is accepted for signature parity; the fan-out runs on the GPU.
+    With device_clock=True every band is rendered by one batch
+    (lpk_generate_scene_to_files: clock walks on the GPU, split fan-out,
+    rounds of round_s seconds written while the next round renders);
+    otherwise band by band with the host clock stream."""
     os.makedirs(directory, exist_ok=True)
     p = Prepared(scene, ctx)
     out = []
+    if device_clock:
+        names = [f"{scene.receivers[r].name}__{scene.receivers[r].bands[b].band_id}" for (r, b) in p.work()]
+        paths = [os.path.join(directory, f"{nm}.iq.c64") for nm in names]
+        arr = (C.c_char_p * len(paths))(*[x.encode() for x in paths])
+        flags = (N.LPK_NOISE_ON if noise else N.LPK_NOISE_OFF) | N.LPK_GEN_DEVICE_CLOCK | N.LPK_GEN_SPLIT
+        N.check(N.lib().lpk_generate_scene_to_files(p.h, rng_seed_base & 0xFFFFFFFFFFFFFFFF, float(round_s), flags,
+                                                     arr), p.ctx.h)
+        for (r, b), nm, path in zip(p.work(), names, paths):
+            band = scene.receivers[r].bands[b]
+            n = p.n_samples(r, b)
+            desc = p.band_meta(r, b, p.active(r, b))
+            write_sidecar(directory, nm, scene.epoch_unix, band.sample_rate_hz, band.lo_carrier_hz, n, desc)
+            out.append(OutputManifest(nm, path, n, desc))
+        p.close()
+        return out
     for work_idx, (r, b) in enumerate(p.work()):
         rx = scene.receivers[r]
         band = rx.bands[b]

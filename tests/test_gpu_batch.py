@@ -269,3 +269,21 @@ def test_full_scene_split_batch_matches_fp64_batch(ctx):
         assert r <= 1e-5, (u, r)
     print(f"full 120 s scene, batched split vs batched FP64: worst IQ error {worst:.2e} of max")
     prep.close()
+
+
+def test_scene_to_dir_through_the_batch(ctx, tmp_path):
+    """run_scene_to_dir on the batch (lpk_generate_scene_to_files): each
+    band's .iq.c64 holds exactly what lpk_generate_scene hands its sink, and
+    every band has its sidecar."""
+    sc = scenes.config_c1(duration_s=3.0)
+    man = P.run_scene_to_dir(sc, 4242, str(tmp_path), ctx=ctx, device_clock=True, round_s=1.0)
+    prep = P.Prepared(sc, ctx)
+    got = {}
+    prep.generate_scene(4242, 1.0, lambda w, c: got.setdefault(w, []).append(c) and False)
+    assert len(man) == len(prep.work()) == len(got)
+    for w, m in enumerate(man):
+        data = np.fromfile(m.path, dtype=np.complex64)
+        assert data.size == m.n_samples == prep.n_samples(*prep.work()[w]) > 0
+        assert data.tobytes() == np.concatenate(got[w]).tobytes()
+        assert (tmp_path / f"{m.name}.iq.json").exists()
+    prep.close()
