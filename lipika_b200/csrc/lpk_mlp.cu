@@ -51,20 +51,32 @@ struct __align__(16) MlpWeights {
     float b1[kH], b2[kH], w3[kH], b3;
 };
 
+// Weight gradients of one block step as one tcgen05 product, K = the
+// step's 128 rows: A = [dZ2^T; dZ1^T] (128 x 128), B = [H1^T; X^T; 0]
+// (80 x 128), so D = A B^T holds dW2 = dZ2^T H1 in rows 0-63 / columns 0-63
+// and dW1 = dZ1^T X in rows 64-127 / columns 64-71 (the other blocks are
+// not used). Both operands in the no-swizzle K-major core-matrix layout
+// (element (row, k) at [k / 8][row][k % 8]).
+constexpr int kGradN = 80;
+constexpr uint32_t kGradCols = 128;  // TMEM columns (a power of two >= kGradN)
+constexpr uint32_t kGradIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kGradN >> 3) << 17) |
+                                ((uint32_t)(kRowsPerBlock >> 4) << 24);
+
 struct __align__(16) MlpTiles {  // one block step of 128 rows (training)
-    __nv_bfloat16 x[kRowsPerBlock][kLdX];
-    __nv_bfloat16 h1[kRowsPerBlock][kLdH];
-    __nv_bfloat16 dz1[kRowsPerBlock][kLdH];
-    __nv_bfloat16 dz2[kRowsPerBlock][kLdH];
+    __nv_bfloat16 ga[kRowsPerBlock / 8][2 * kH][8];
+    __nv_bfloat16 gb[kRowsPerBlock / 8][kGradN][8];
     float db1[kH], db2[kH], dw3[kH], db3, loss;
+    unsigned long long bar;
+    uint32_t tmem;
 };
+// At most four gradient CTAs (their weights and tiles) fit on an SM's
+// 228 KB, so their TMEM (4 x 128 columns) never exceeds the SM's 512.
+static_assert(5 * (sizeof(MlpWeights) + sizeof(MlpTiles)) > 228 * 1024 && 4 * kGradCols <= 512,
+              "TMEM residency bound");
 
 __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
     __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
     return *reinterpret_cast<uint32_t *>(&v);
-}
-__device__ __forceinline__ uint32_t pack2h(__nv_bfloat16 lo, __nv_bfloat16 hi) {
-    return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
 }
 __device__ __forceinline__ uint32_t ld2(const __nv_bfloat16 *p) { return *reinterpret_cast<const uint32_t *>(p); }
 
@@ -152,6 +164,104 @@ __device__ __forceinline__ float2 load_x2(const float *__restrict__ x, int64_t r
     return make_float2(x[row * kF + 2 * tig], x[row * kF + 2 * tig + 1]);
 }
 
+constexpr int kTcRows = 128;          // rows per tile = the MMA's M
+constexpr uint32_t kTcCols = 64;      // TMEM columns: one 128 x 64 FP32 accumulator, reused by both layers
+// kind::f16 instruction descriptor: FP32 accumulator (bits 4-5 = 1), BF16 A
+// (7-9 = 1) and B (10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at 24.
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kH >> 3) << 17) |
+                              ((uint32_t)(kTcRows >> 4) << 24);
+constexpr int kTcSpin = 1 << 20;      // mbarrier polls before a wait gives up
+
+struct __align__(1024) TcSmem {
+    __nv_bfloat16 a1[2][kTcRows][8];  // x tile, K padded to 16: column groups 0-7 and 8-15 (zero)
+    __nv_bfloat16 a2[kH / 8][kTcRows][8];  // first hidden layer, 8 column groups
+    __nv_bfloat16 b1[2][kH][8];       // W1 (out x in), K padded to 16
+    __nv_bfloat16 b2[kH / 8][kH][8];  // W2 (out x in)
+    float bias1[kH], bias2[kH], w3[kH];
+    float b3;
+    unsigned long long bar;
+    uint32_t tmem;
+};
+// At most 7 CTAs of 29 KB or more fit on an SM (228 KB), so their TMEM
+// demand (7 x 64 columns) stays within the SM's 512 and tcgen05.alloc never
+// waits on another CTA.
+static_assert(sizeof(TcSmem) >= 29 * 1024 && 7 * kTcCols <= 512, "TMEM residency bound");
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor (no swizzle, K-major): start address,
+// leading byte offset (next 8 K-elements), stride byte offset (next 8 rows),
+// all in 16-byte units; version 1 (bit 46); base offset, LBO mode and layout
+// type 0.
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate,
+                                       uint32_t idesc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t phase) {
+    for (int it = 0; it < kTcSpin; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// This warp's 32 accumulator rows (lane = row), 64 FP32 columns.
+__device__ __forceinline__ void tc_load_row(uint32_t taddr, float v[kH]) {
+#pragma unroll
+    for (int q = 0; q < kH / 16; ++q) {
+        uint32_t r[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15}, [%16];\n"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr + (uint32_t)(16 * q)));
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[16 * q + i] = __uint_as_float(r[i]);
+    }
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// This warp's 32 accumulator rows, 16 FP32 columns from taddr's column.
+__device__ __forceinline__ void tc_load16(uint32_t taddr, float v[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 // Sum of v over the 16 rows a warp holds (rows g and g+8 of every group):
 // this thread's two elements, then across the eight groups.
 __device__ __forceinline__ float rows_sum(float a, float b) {
@@ -170,19 +280,38 @@ __device__ __forceinline__ float rows_sum(float a, float b) {
 // 128 rows (dW2: 32 tiles of 16x8, four per warp; dW1: 4 tiles).
 __global__ void __launch_bounds__(256) k_mlp_grad(const float *__restrict__ p, const float *__restrict__ x,
                                                   const float *__restrict__ t, int64_t n, float two_over_n,
-                                                  float *__restrict__ grad, float *__restrict__ loss) {
+                                                  float *__restrict__ grad, float *__restrict__ loss,
+                                                  int *__restrict__ err) {
     __shared__ MlpWeights S;
     extern __shared__ __align__(16) unsigned char tiles_raw[];
     MlpTiles &T = *reinterpret_cast<MlpTiles *>(tiles_raw);
     stage_weights(p, S);
-    for (int i = threadIdx.x; i < kRowsPerBlock * kLdX; i += blockDim.x)
-        T.x[i / kLdX][i % kLdX] = __float2bfloat16_rn(0.0f);
+    for (int i = threadIdx.x; i < (kRowsPerBlock / 8) * (kGradN - kH - kF) * 8; i += blockDim.x) {
+        const int kg = i / ((kGradN - kH - kF) * 8), rest = i % ((kGradN - kH - kF) * 8);
+        T.gb[kg][kH + kF + rest / 8][rest % 8] = __float2bfloat16_rn(0.0f);  // B rows 72-79 stay zero
+    }
     for (int i = threadIdx.x; i < kH; i += blockDim.x) T.db1[i] = T.db2[i] = T.dw3[i] = 0.0f;
-    if (threadIdx.x == 0) T.db3 = T.loss = 0.0f;
-    __syncthreads();
+    if (threadIdx.x == 0) {
+        T.db3 = T.loss = 0.0f;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&T.bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane >> 2, tig = lane & 3;
-    float dw2[4][4] = {}, dw1[4] = {};
-    for (int64_t r0 = (int64_t)blockIdx.x * kRowsPerBlock; r0 < n; r0 += (int64_t)gridDim.x * kRowsPerBlock) {
+    if (w == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&T.tmem)),
+                     "r"(kGradCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = T.tmem, bar = smem_u32(&T.bar);
+    uint32_t phase = 0;
+    bool ok = true;
+    int64_t steps = 0;
+    for (int64_t r0 = (int64_t)blockIdx.x * kRowsPerBlock; r0 < n && ok;
+         r0 += (int64_t)gridDim.x * kRowsPerBlock, ++steps) {
         const int64_t ra = r0 + 16 * w + g, rb = ra + 8;
         const float2 xa = load_x2(x, ra, n, tig), xb = load_x2(x, rb, n, tig);
         WarpAct A;
@@ -242,63 +371,74 @@ __global__ void __launch_bounds__(256) k_mlp_grad(const float *__restrict__ p, c
                 const float s1 = rows_sum(dz1[e], dz1[e + 2]);
                 if (g == 0) atomicAdd(&T.db1[8 * j + 2 * tig + e], s1);
             }
+            // operands of the weight gradients, transposed into the K-major
+            // tiles (K = the step's row): rows ra_s / rb_s, columns c, c + 1
             const int c = 8 * j + 2 * tig;
-            *reinterpret_cast<uint32_t *>(&T.dz1[ra_s][c]) = pack2(dz1[0], dz1[1]);
-            *reinterpret_cast<uint32_t *>(&T.dz1[rb_s][c]) = pack2(dz1[2], dz1[3]);
-            *reinterpret_cast<uint32_t *>(&T.dz2[ra_s][c]) = pack2(dz2[j][0], dz2[j][1]);
-            *reinterpret_cast<uint32_t *>(&T.dz2[rb_s][c]) = pack2(dz2[j][2], dz2[j][3]);
-            *reinterpret_cast<uint32_t *>(&T.h1[ra_s][c]) = pack2(A.h1[j][0], A.h1[j][1]);
-            *reinterpret_cast<uint32_t *>(&T.h1[rb_s][c]) = pack2(A.h1[j][2], A.h1[j][3]);
+            T.ga[ra_s >> 3][c][ra_s & 7] = __float2bfloat16_rn(dz2[j][0]);
+            T.ga[ra_s >> 3][c + 1][ra_s & 7] = __float2bfloat16_rn(dz2[j][1]);
+            T.ga[rb_s >> 3][c][rb_s & 7] = __float2bfloat16_rn(dz2[j][2]);
+            T.ga[rb_s >> 3][c + 1][rb_s & 7] = __float2bfloat16_rn(dz2[j][3]);
+            T.ga[ra_s >> 3][kH + c][ra_s & 7] = __float2bfloat16_rn(dz1[0]);
+            T.ga[ra_s >> 3][kH + c + 1][ra_s & 7] = __float2bfloat16_rn(dz1[1]);
+            T.ga[rb_s >> 3][kH + c][rb_s & 7] = __float2bfloat16_rn(dz1[2]);
+            T.ga[rb_s >> 3][kH + c + 1][rb_s & 7] = __float2bfloat16_rn(dz1[3]);
+            T.gb[ra_s >> 3][c][ra_s & 7] = __float2bfloat16_rn(A.h1[j][0]);
+            T.gb[ra_s >> 3][c + 1][ra_s & 7] = __float2bfloat16_rn(A.h1[j][1]);
+            T.gb[rb_s >> 3][c][rb_s & 7] = __float2bfloat16_rn(A.h1[j][2]);
+            T.gb[rb_s >> 3][c + 1][rb_s & 7] = __float2bfloat16_rn(A.h1[j][3]);
         }
-        *reinterpret_cast<uint32_t *>(&T.x[ra_s][2 * tig]) = pack2(xa.x, xa.y);
-        *reinterpret_cast<uint32_t *>(&T.x[rb_s][2 * tig]) = pack2(xb.x, xb.y);
+        T.gb[ra_s >> 3][kH + 2 * tig][ra_s & 7] = __float2bfloat16_rn(xa.x);
+        T.gb[ra_s >> 3][kH + 2 * tig + 1][ra_s & 7] = __float2bfloat16_rn(xa.y);
+        T.gb[rb_s >> 3][kH + 2 * tig][rb_s & 7] = __float2bfloat16_rn(xb.x);
+        T.gb[rb_s >> 3][kH + 2 * tig + 1][rb_s & 7] = __float2bfloat16_rn(xb.y);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // generic writes -> the MMA's reads
+        tc_fence_before();
         __syncthreads();
-        // weight gradients over the block's 128 rows: dW2 = dZ2ᵀ H1, dW1 = dZ1ᵀ X
+        // weight gradients over the block's 128 rows, accumulated in TMEM
+        // over the block's steps: eight K = 16 MMAs of M = 128, N = 80
+        if (threadIdx.x == 0) {
+            tc_fence_after();
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int tt = 4 * w + q, mi = tt >> 3, nj = tt & 7;
-#pragma unroll
-            for (int kb = 0; kb < kRowsPerBlock / 16; ++kb) {
-                const int k0 = 16 * kb + 2 * tig, m0 = 16 * mi + g, n0 = 8 * nj + g;
-                const uint32_t a[4] = {pack2h(T.dz2[k0][m0], T.dz2[k0 + 1][m0]),
-                                       pack2h(T.dz2[k0][m0 + 8], T.dz2[k0 + 1][m0 + 8]),
-                                       pack2h(T.dz2[k0 + 8][m0], T.dz2[k0 + 9][m0]),
-                                       pack2h(T.dz2[k0 + 8][m0 + 8], T.dz2[k0 + 9][m0 + 8])};
-                mma16816(dw2[q], a, pack2h(T.h1[k0][n0], T.h1[k0 + 1][n0]),
-                         pack2h(T.h1[k0 + 8][n0], T.h1[k0 + 9][n0]));
-            }
+            for (int kk = 0; kk < kRowsPerBlock / 16; ++kk)
+                tc_mma(tmem, tc_desc(smem_u32(&T.ga[2 * kk][0][0]), 2 * kH * 16, 128),
+                       tc_desc(smem_u32(&T.gb[2 * kk][0][0]), kGradN * 16, 128),
+                       (steps > 0 || kk > 0) ? 1u : 0u, kGradIdesc);
+            tc_commit(bar);
         }
-        if ((w & 1) == 0) {
-            const int mi = w >> 1;
-#pragma unroll
-            for (int kb = 0; kb < kRowsPerBlock / 16; ++kb) {
-                const int k0 = 16 * kb + 2 * tig, m0 = 16 * mi + g;
-                const uint32_t a[4] = {pack2h(T.dz1[k0][m0], T.dz1[k0 + 1][m0]),
-                                       pack2h(T.dz1[k0][m0 + 8], T.dz1[k0 + 1][m0 + 8]),
-                                       pack2h(T.dz1[k0 + 8][m0], T.dz1[k0 + 9][m0]),
-                                       pack2h(T.dz1[k0 + 8][m0 + 8], T.dz1[k0 + 9][m0 + 8])};
-                mma16816(dw1, a, pack2h(T.x[k0][g], T.x[k0 + 1][g]), pack2h(T.x[k0 + 8][g], T.x[k0 + 9][g]));
-            }
-        }
+        ok = __syncthreads_and(tc_wait(bar, phase));  // the tiles are rewritten by the next step
+        phase ^= 1u;
+        tc_fence_after();
         __syncthreads();  // the next step overwrites the tiles
     }
+    if (!ok && threadIdx.x == 0 && err) atomicOr(err, 1);
+    // Warps w and w + 4 share TMEM lane quarter w % 4 (accumulator rows
+    // 32 (w % 4) ..): quarters 0-1 hold dW2, each warp of the pair reading
+    // 32 of its 64 columns; quarters 2-3 hold dW1 in columns 64-71.
+    const int q = w & 3, half = w >> 2;
+    if (ok && steps > 0 && (q < 2 || half == 0)) {
+        const uint32_t taddr = tmem + ((uint32_t)(32 * q) << 16);
+        const int m = 32 * q + lane;
+        float v[16];
+        if (q < 2) {
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int tt = 4 * w + q, mi = tt >> 3, nj = tt & 7;
-        const int row = 16 * mi + g, col = 8 * nj + 2 * tig;
-        atomicAdd(&grad[kOffW2 + row * kH + col], dw2[q][0]);
-        atomicAdd(&grad[kOffW2 + row * kH + col + 1], dw2[q][1]);
-        atomicAdd(&grad[kOffW2 + (row + 8) * kH + col], dw2[q][2]);
-        atomicAdd(&grad[kOffW2 + (row + 8) * kH + col + 1], dw2[q][3]);
+            for (int part = 0; part < 2; ++part) {
+                const int c0 = 32 * half + 16 * part;
+                tc_load16(taddr + (uint32_t)c0, v);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) atomicAdd(&grad[kOffW2 + m * kH + c0 + i], v[i]);
+            }
+        } else {
+            tc_load16(taddr + (uint32_t)kH, v);
+#pragma unroll
+            for (int f = 0; f < kF; ++f) atomicAdd(&grad[kOffW1 + (m - kH) * kF + f], v[f]);
+        }
     }
-    if ((w & 1) == 0) {
-        const int row = 16 * (w >> 1) + g, col = 2 * tig;  // input columns 0..7 only
-        atomicAdd(&grad[kOffW1 + row * kF + col], dw1[0]);
-        atomicAdd(&grad[kOffW1 + row * kF + col + 1], dw1[1]);
-        atomicAdd(&grad[kOffW1 + (row + 8) * kF + col], dw1[2]);
-        atomicAdd(&grad[kOffW1 + (row + 8) * kF + col + 1], dw1[3]);
-    }
+    tc_fence_before();
     __syncthreads();
+    if (w == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kGradCols) : "memory");
+    }
     for (int i = threadIdx.x; i < kH; i += blockDim.x) {
         atomicAdd(&grad[kOffB1 + i], T.db1[i]);
         atomicAdd(&grad[kOffB2 + i], T.db2[i]);
@@ -490,89 +630,6 @@ __global__ void k_mlp_normalize(float *__restrict__ x, float *__restrict__ y, in
 // the mma.sync kernels (BF16 x, W1, W2 and first hidden layer; FP32
 // accumulation and everything else), so the CPU restatement covers both;
 // only the FP32 summation order differs (bias added after the products).
-constexpr int kTcRows = 128;          // rows per tile = the MMA's M
-constexpr uint32_t kTcCols = 64;      // TMEM columns: one 128 x 64 FP32 accumulator, reused by both layers
-// kind::f16 instruction descriptor: FP32 accumulator (bits 4-5 = 1), BF16 A
-// (7-9 = 1) and B (10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at 24.
-constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kH >> 3) << 17) |
-                              ((uint32_t)(kTcRows >> 4) << 24);
-constexpr int kTcSpin = 1 << 20;      // mbarrier polls before a wait gives up
-
-struct __align__(1024) TcSmem {
-    __nv_bfloat16 a1[2][kTcRows][8];  // x tile, K padded to 16: column groups 0-7 and 8-15 (zero)
-    __nv_bfloat16 a2[kH / 8][kTcRows][8];  // first hidden layer, 8 column groups
-    __nv_bfloat16 b1[2][kH][8];       // W1 (out x in), K padded to 16
-    __nv_bfloat16 b2[kH / 8][kH][8];  // W2 (out x in)
-    float bias1[kH], bias2[kH], w3[kH];
-    float b3;
-    unsigned long long bar;
-    uint32_t tmem;
-};
-// At most 7 CTAs of 29 KB or more fit on an SM (228 KB), so their TMEM
-// demand (7 x 64 columns) stays within the SM's 512 and tcgen05.alloc never
-// waits on another CTA.
-static_assert(sizeof(TcSmem) >= 29 * 1024 && 7 * kTcCols <= 512, "TMEM residency bound");
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-// Shared-memory matrix descriptor (no swizzle, K-major): start address,
-// leading byte offset (next 8 K-elements), stride byte offset (next 8 rows),
-// all in 16-byte units; version 1 (bit 46); base offset, LBO mode and layout
-// type 0.
-__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
-}
-
-__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
-        :
-        : "r"(tmem_d), "l"(da), "l"(db), "r"(kTcIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-}
-
-__device__ __forceinline__ void tc_commit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t phase) {
-    for (int it = 0; it < kTcSpin; ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(bar), "r"(phase)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-// This warp's 32 accumulator rows (lane = row), 64 FP32 columns.
-__device__ __forceinline__ void tc_load_row(uint32_t taddr, float v[kH]) {
-#pragma unroll
-    for (int q = 0; q < kH / 16; ++q) {
-        uint32_t r[16];
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-            "%14, %15}, [%16];\n"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-            : "r"(taddr + (uint32_t)(16 * q)));
-#pragma unroll
-        for (int i = 0; i < 16; ++i) v[16 * q + i] = __uint_as_float(r[i]);
-    }
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
 // y = MLP(x) for n rows of normalised features; err (may be NULL) gets 1 if
 // an MMA completion wait gave up (the outputs are then incomplete).
 __global__ void __launch_bounds__(128, 1) k_mlp_forward_tc(const float *__restrict__ p, const float *__restrict__ x,
@@ -635,7 +692,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward_tc(const float *__restri
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
-            tc_mma(tmem, d_a1, d_b1, 0u);  // layer 1: one K = 16 step
+            tc_mma(tmem, d_a1, d_b1, 0u, kTcIdesc);  // layer 1: one K = 16 step
             tc_commit(bar);
         }
         ok = __syncthreads_and(tc_wait(bar, phase));
@@ -661,7 +718,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward_tc(const float *__restri
 #pragma unroll
             for (int kk = 0; kk < kH / 16; ++kk)  // layer 2: four K = 16 steps
                 tc_mma(tmem, tc_desc(smem_u32(&S.a2[2 * kk][0][0]), kTcRows * 16, 128),
-                       tc_desc(smem_u32(&S.b2[2 * kk][0][0]), kH * 16, 128), kk > 0 ? 1u : 0u);
+                       tc_desc(smem_u32(&S.b2[2 * kk][0][0]), kH * 16, 128), kk > 0 ? 1u : 0u, kTcIdesc);
             tc_commit(bar);
         }
         ok = __syncthreads_and(tc_wait(bar, phase));
@@ -706,6 +763,7 @@ using namespace lpk;
 struct lpk_mlp {
     lpk_ctx *ctx = nullptr;
     float *d_p = nullptr, *d_m = nullptr, *d_v = nullptr, *d_g = nullptr, *d_norm = nullptr;
+    int *d_err = nullptr;  // set by the gradient kernel when a tensor-core completion wait gives up
     float norm[2 * kF + 2];  // feature means, feature stds, target mean, target std (µs)
     int64_t step = 0;
 };
@@ -727,7 +785,8 @@ lpk_status launch_grad(lpk_mlp *m, const float *d_x, const float *d_t, int64_t n
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
     const int64_t steps = (n + kRowsPerBlock - 1) / kRowsPerBlock;
     const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>(steps, 2 * sms));
-    k_mlp_grad<<<grid, 256, grad_smem(), c->stream>>>(m->d_p, d_x, d_t, n, 2.0f / (float)n, m->d_g, d_loss);
+    k_mlp_grad<<<grid, 256, grad_smem(), c->stream>>>(m->d_p, d_x, d_t, n, 2.0f / (float)n, m->d_g, d_loss,
+                                                      m->d_err);
     e = cudaGetLastError();
     c->launches += 1;
     return e == cudaSuccess ? LPK_OK : cuda_fail(c, e, "mlp gradient kernel");
@@ -756,6 +815,11 @@ lpk_status lpk_mlp_create(lpk_ctx *c, uint64_t seed, lpk_mlp **out) {
             lpk_mlp_destroy(m);
             return fail(c, LPK_ENOMEM, "mlp allocation failed");
         }
+    }
+    if (cudaMalloc((void **)&m->d_err, sizeof(int)) != cudaSuccess ||
+        cudaMemset(m->d_err, 0, sizeof(int)) != cudaSuccess) {
+        lpk_mlp_destroy(m);
+        return fail(c, LPK_ENOMEM, "mlp allocation failed");
     }
     // Glorot-uniform weights from a SplitMix64 stream, zero biases
     std::vector<float> p(kParams, 0.0f);
@@ -798,6 +862,7 @@ void lpk_mlp_destroy(lpk_mlp *m) {
     cudaStreamSynchronize(m->ctx->stream);
     for (float *p : {m->d_p, m->d_m, m->d_v, m->d_g, m->d_norm})
         if (p) cudaFree(p);
+    if (m->d_err) cudaFree(m->d_err);
     delete m;
 }
 
@@ -877,8 +942,11 @@ lpk_status lpk_mlp_loss_grad(lpk_mlp *m, const float *x, const float *t, int64_t
     if (e == cudaSuccess && grad)
         e = cudaMemcpyAsync(grad, m->d_g, sizeof(float) * kParams, cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(m->d_g, 0, sizeof(float) * kParams, c->stream);
+    int herr = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, m->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "mlp gradient read");
+    if (herr) return fail(c, LPK_ETIMEDOUT, "mlp gradient: a tensor-core completion wait gave up");
     if (loss) *loss = (double)l / (double)n;
     return LPK_OK;
 }
@@ -969,9 +1037,15 @@ lpk_status lpk_mlp_fit(lpk_mlp *m, int32_t tx, const double *rx, double epoch, d
         if (e != cudaSuccess) s = cuda_fail(c, e, "loss curve");
         for (int32_t k = 0; k < steps && !s; ++k) loss_curve[k] /= (float)batch;
     }
-    e = cudaGetLastError();
+    int herr = 0;
+    if (!s) {
+        e = cudaMemcpyAsync(&herr, m->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) s = cuda_fail(c, e, "mlp training");
+    }
+    if (!s && (e = cudaGetLastError()) != cudaSuccess) s = cuda_fail(c, e, "mlp training");
     cleanup();
-    if (!s && e != cudaSuccess) s = cuda_fail(c, e, "mlp training");
+    if (!s && herr) s = fail(c, LPK_ETIMEDOUT, "mlp training: a tensor-core completion wait gave up");
     return s;
 }
 
