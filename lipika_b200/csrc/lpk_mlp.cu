@@ -16,11 +16,12 @@
 // converged delay is reported (the surrogate is judged, never trusted).
 //
 // The network is trained on this GPU from delays the converged solver
-// itself produces, by the kernels below: training's forward, backward and
-// weight gradients run as BF16 mma.sync tiles with FP32 accumulation (16- to
-// 64-wide products inside one warp's registers); inference runs on the
-// 5th-generation tensor cores (tcgen05.mma, accumulator in TMEM, 128-row
-// tiles); Adam updates FP32 master weights. Rounding points (BF16:
+// itself produces, by the kernels below: inference and training's weight
+// gradients run on the 5th-generation tensor cores (tcgen05.mma, BF16
+// operands, FP32 accumulator in TMEM, 128-row tiles); training's forward
+// and backward dH1 run as BF16 mma.sync tiles inside each warp's registers
+// (16- to 64-wide products between layers); Adam updates FP32 master
+// weights. Rounding points (BF16:
 // inputs, W1, W2, the first hidden layer and the two pre-activation
 // gradients; everything else FP32) are restated in oracle/mlp_ref.py.
 #include <algorithm>
