@@ -369,8 +369,9 @@ lpk_status lpk_solve_features(lpk_ctx *ctx, int32_t tx, const double *rx_ecef, d
 /* A tanh MLP 8 -> 64 -> 64 -> 1 whose output, de-normalised, is the
  * light-time correction tau - R/c in microseconds. Glorot-uniform initial
  * weights from `seed`. Forward, backward and the weight gradients run on
- * the tensor cores with BF16 operands and FP32 accumulation (inference on
- * tcgen05 with a TMEM accumulator, training as mma.sync tiles); Adam
+ * the tensor cores with BF16 operands and FP32 accumulation (inference and
+ * the weight gradients on tcgen05 with a TMEM accumulator, training's
+ * forward and backward activations as register mma.sync tiles); Adam
  * updates FP32 master weights. */
 lpk_status lpk_mlp_create(lpk_ctx *ctx, uint64_t seed, lpk_mlp **out);
 void lpk_mlp_destroy(lpk_mlp *mlp);
