@@ -76,8 +76,10 @@ struct __align__(16) AnchorRec {
     int32_t flags;
     int32_t nav_pm;                   // nav sign of the tile (1 with nav off; unused with kRecNavVary)
     int64_t sym_raw0, sym_pos0;       // framed kinds: raw symbol count at the tile start and its frame slot
-    double chip_fl0;                  // C/A: a whole chip count at or below the tile's first chip
-    int32_t chip_m0;                  // C/A: chip_fl0 mod 1023
+    double chip_base;                 // C/A: 1.5 x 2^52 - f0, f0 a whole chip count at or below the
+                                      // tile's first chip (floor(cp) + chip_base holds floor(cp) - f0
+                                      // in its low 32 bits, exactly)
+    int32_t chip_m0;                  // C/A: f0 mod 1023
     int32_t n_nodes;                  // most grid nodes either iterate crosses in the tile
 };
 static_assert(sizeof(AnchorRec) % 16 == 0, "AnchorRec arrays must keep 16-byte alignment");
@@ -203,7 +205,7 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
         r.k1[p] = 0.0;
         for (int i = 0; i < 3; ++i) r.p0[p][i] = r.p1[p][i] = 0.0;
     }
-    r.chip_fl0 = 0.0;
+    r.chip_base = 0.0;
     r.chip_m0 = 0;
     if (exact_only) {
         r.amp0 = r.amp1 = 0.0f;
@@ -321,13 +323,13 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
             if (tx.has_repeat && !((te_e - te_s) * tx.rate + 3.0 < (double)tx.n_sym)) exact = true;
         }
     }
-    if (!exact && tx.sig_kind == kCa) {  // tile-relative chip index: chip_m0 + (floor(cp) - chip_fl0)
+    if (!exact && tx.sig_kind == kCa) {  // tile-relative chip index: chip_m0 + (floor(cp) - f0)
         const double cs = (te_s - tx.epoch_rel) * kCaChipRate, ce = (te_e - tx.epoch_rel) * kCaChipRate;
         const double f0 = floor(cs) - 2.0;
         if (!(fabs(f0) < 1.0e15) || !(ce - f0 + 2.0 < 1023.0)) {
             r.flags |= kRecCaWide;
         } else {
-            r.chip_fl0 = f0;
+            r.chip_base = 0x1.8p52 - f0;  // exact: |f0| < 1e15 < 2^50
             r.chip_m0 = (int32_t)i64_rem_euclid((int64_t)f0, 1023);
         }
     }
@@ -413,7 +415,9 @@ __device__ __forceinline__ void split_baseband(const DevTx &tx, const AnchorRec 
         }
         int m;
         if constexpr (K == kPassCa) {  // within [0, 2045) for every sample in the fit range
-            m = R.chip_m0 + (int)(fl - R.chip_fl0);
+            // fl + chip_base = 1.5 x 2^52 + (fl - f0) exactly (|fl - f0| < 2^51):
+            // its low mantissa word is fl - f0, read without a conversion
+            m = R.chip_m0 + __double2loint(__dadd_rn(fl, R.chip_base));
             m -= m >= 1023 ? 1023 : 0;
             m = (unsigned)m < 1023u ? m : 0;  // samples outside the fit range are redone exactly
         } else {
