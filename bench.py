@@ -500,6 +500,9 @@ def _learned_leg(ctx, N, prep, sc):
     evaluations per sample on 100k fresh reception times."""
     d = prep.band_desc(0, 0, 2026, 0)
     rx = np.array(d.rx_ecef[:])
+    warm = N.Mlp(ctx, seed=4)  # first use of the training kernels, untimed
+    warm.fit(0, rx, d.epoch_unix, 0.0, sc.duration_s, n_train=1 << 14, steps=20, batch=4096, lr=3e-3, seed=8)
+    warm.close()
     t0 = time.perf_counter()
     m = N.Mlp(ctx, seed=5)
     curve = m.fit(0, rx, d.epoch_unix, 0.0, sc.duration_s, n_train=1 << 18, steps=1500, batch=4096, lr=3e-3, seed=9)
