@@ -221,3 +221,13 @@ def test_device_tables_flag_needs_a_context_and_known_flags():
     assert N.lib().lpk_scene_prepare(None, C.byref(cs.cfg), C.byref(h)) == N.LPK_EINVAL and not h.value
     cs.cfg.flags = 1 << 5
     assert N.lib().lpk_scene_prepare(None, C.byref(cs.cfg), C.byref(h)) == N.LPK_EINVAL and not h.value
+
+
+def test_new_entry_points_reject_bad_arguments_without_a_gpu():
+    L = N.lib()
+    paths = (C.c_char_p * 1)(b"/nonexistent/x.iq.c64")
+    assert L.lpk_generate_scene_to_files(None, 0, 1.0, 0, paths) == N.LPK_EINVAL
+    o = (N.KeplerOrbit * 1)(N.KeplerOrbit(7e6, 50.0, 0.0, 0.0, 0.0))
+    g = np.zeros(6)
+    assert L.lpk_kepler_tables(None, o, 1, 0.0, 0.01, 2, g.ctypes.data_as(N._D)) == N.LPK_EINVAL
+    assert L.lpk_sample_times(None, 2.048e6, 0, 4, g.ctypes.data_as(N._D)) == N.LPK_EINVAL
