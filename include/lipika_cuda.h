@@ -209,18 +209,39 @@ lpk_status lpk_band_chunk_device(lpk_ctx *ctx, const lpk_band_desc *band, const 
                                  const double *d_rx_pos3n, lpk_cf32 *d_out, uint8_t *d_unoccluded);
 lpk_status lpk_sync(lpk_ctx *ctx);
 
+/* Accuracy of the split-precision fan-out (no reference counterpart; the
+ * reference has one all-FP64 path). Renders band samples [i0, i0 + n) of a
+ * band with solver LPK_SOLVER_SPLIT and a stationary receiver exactly as
+ * lpk_band_chunk_device does (into d_out, DEVICE memory, when not NULL),
+ * and for every (sample, transmitter) the split path evaluates on its fast
+ * path also runs the reference-exact FP64 solve and phase (the arithmetic
+ * of the all-FP64 kernel, src/channel/mod.rs:70-99, :251-267): returns the
+ * largest |delay difference| (s) and |carrier-phase difference| (rad,
+ * wrapped to [-pi, pi]) over them, the number of fast-path (sample,
+ * transmitter) pairs compared and the number taken on the exact path
+ * (which equal the FP64 kernel's by construction). Synchronous. */
+lpk_status lpk_split_accuracy(lpk_ctx *ctx, const lpk_band_desc *band, const int32_t *active_tx, int32_t n_active,
+                              int64_t i0, int64_t n, const double *d_delta_t, lpk_cf32 *d_out,
+                              double *max_delay_err_s, double *max_phase_err_rad, int64_t *n_fast, int64_t *n_exact);
+
 /* lpk_band_chunk_device for callers that cannot allocate device memory when
  * they render (a real-time thread that must not stall on the CUDA allocator,
  * a host that reserved the device for its own pool). No counterpart in the
  * reference. It calls no cudaMalloc/cudaFree: its working memory is one
- * file-scope static device array of 10 MiB that every GPU loading this
- * library holds until exit. Limits: at most 256 active transmitters; with
- * LPK_CLOCK_DEVICE_WALK a chunk may span at most 2^20 master-clock samples
- * and lie within the first 2^29 (larger requests return LPK_EINVAL). The
- * first call on a device looks up the array's address (cudaGetSymbolAddress)
- * — make that first call before any stream capture. All calls share the
- * array: calls that overlap on the GPU race; each call re-clears what it
- * needs zeroed. Outputs equal lpk_band_chunk_device's. */
+ * file-scope static device array of 22 MiB that every GPU loading this
+ * library holds until exit. It runs the kernels lpk_band_chunk_device runs
+ * for the band's solver (the split path for LPK_SOLVER_SPLIT with a
+ * stationary receiver, the FP64 kernel otherwise) on the same inputs, so
+ * its outputs equal lpk_band_chunk_device's bit for bit. Limits: at most
+ * 256 active transmitters; with LPK_CLOCK_DEVICE_WALK a chunk may span at
+ * most 2^20 master-clock samples and lie within the first 2^29; a split
+ * chunk may need at most 32,768 (tile, transmitter) anchor records (larger
+ * requests return LPK_EINVAL). Every call rebuilds the clock walk's block
+ * totals and carries from master sample 0, so its walk work grows with the
+ * chunk's master-sample offset. The first call on a device looks up the
+ * array's address (cudaGetSymbolAddress) — make that first call before any
+ * stream capture. All calls share the array: calls that overlap on the GPU
+ * race; each call re-clears what it needs zeroed. */
 lpk_status lpk_band_chunk_device_static(lpk_ctx *ctx, const lpk_band_desc *band, const int32_t *active_tx,
                                         int32_t n_active, int64_t i0, int64_t n, const double *d_delta_t,
                                         const double *d_rx_pos3n, lpk_cf32 *d_out, uint8_t *d_unoccluded);

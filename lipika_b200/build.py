@@ -10,6 +10,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -38,21 +39,24 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return OUT
     os.makedirs(BUILD, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     inc = ["-I" + os.path.join(HERE, "..", "include")]
     for f in CU:
         o = os.path.join(BUILD, f + ".o")
         extra = os.environ.get("LPK_NVCC_FLAGS", "").split()  # e.g. tile-shape sweeps
-        cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
-               "-Xptxas", "-v" if verbose else "-O3", *extra, *inc, "-c", os.path.join(CSRC, f), "-o", o]
-        subprocess.run(cmd, check=True)
+        cmds.append([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
+                     "-Xptxas", "-v" if verbose else "-O3", *extra, *inc, "-c", os.path.join(CSRC, f), "-o", o])
         objs.append(o)
     for f in CPP:
         o = os.path.join(BUILD, f + ".o")
-        cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
-               "-I/usr/local/cuda/include", *inc, "-c", os.path.join(CSRC, f), "-o", o]
-        subprocess.run(cmd, check=True)
+        cmds.append(["g++", "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
+                     "-I/usr/local/cuda/include", *inc, "-c", os.path.join(CSRC, f), "-o", o])
         objs.append(o)
+    # translation units compile independently: one process each, in parallel
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+        for r in list(pool.map(lambda c: subprocess.run(c), cmds)):
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     tmp = OUT + ".tmp"
     subprocess.run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs], check=True)
     os.replace(tmp, OUT)

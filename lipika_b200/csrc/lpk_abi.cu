@@ -640,6 +640,59 @@ lpk_status lpk_band_chunk_device(lpk_ctx *c, const lpk_band_desc *band, const in
     return LPK_OK;
 }
 
+lpk_status lpk_split_accuracy(lpk_ctx *c, const lpk_band_desc *band, const int32_t *active, int32_t n_active,
+                              int64_t i0, int64_t n, const double *d_delta, lpk_cf32 *d_out, double *max_delay_err_s,
+                              double *max_phase_err_rad, int64_t *n_fast, int64_t *n_exact) {
+    if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
+    if (!band || band->solver != LPK_SOLVER_SPLIT || band->rx_kind != LPK_RX_STATIONARY)
+        return fail(c, LPK_EINVAL, "accuracy mode needs a split-solver band with a stationary receiver");
+    if (!max_delay_err_s || !max_phase_err_rad || !n_fast || !n_exact)
+        return fail(c, LPK_EINVAL, "accuracy outputs are NULL");
+    DevBand b;
+    lpk_status st = build_dev_band(c, band, i0, n, b);
+    if (st) return st;
+    if ((st = check_active(c, active, n_active))) return st;
+    if (b.clock_mode == LPK_CLOCK_HOST && n > 0 && !d_delta) return fail(c, LPK_EINVAL, "delta_t is NULL");
+    b.delta = d_delta;
+    cudaSetDevice(c->device);
+    const size_t off_stats = align256(sizeof(int32_t) * 256);
+    const size_t off_out = off_stats + 256;
+    const size_t off_eps = off_out + (d_out ? 0 : align256(sizeof(float2) * (size_t)(n > 0 ? n : 0)));
+    int64_t kA = 0, span = b.clock_mode == LPK_CLOCK_DEVICE_WALK ? walk_span(band, i0, n, &kA) : 0;
+    const size_t off_recs = off_eps + align256(sizeof(double) * (size_t)span);
+    if ((st = ensure_scratch(c, off_recs + align256(split_recs_bytes(c->split_variant, i0, n, n_active)))))
+        return st;
+    char *base = (char *)c->d_scratch;
+    int32_t *d_active = (int32_t *)base;
+    unsigned long long *d_stats = (unsigned long long *)(base + off_stats);
+    float2 *out = d_out ? (float2 *)d_out : (float2 *)(base + off_out);
+    cudaError_t e = cudaMemcpyAsync(d_active, active, sizeof(int32_t) * (size_t)n_active, cudaMemcpyHostToDevice,
+                                    c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_stats, 0, 4 * sizeof(unsigned long long), c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "accuracy setup");
+    if ((e = split_fork_anchor(c, b, d_active, n_active, base + off_recs)) != cudaSuccess)
+        return cuda_fail(c, e, "anchor fits");
+    if (span && (st = prepare_walk(c, band, i0, n, b, (double *)(base + off_eps), span))) return st;
+    if ((e = cudaStreamWaitEvent(c->stream, c->ev_join, 0)) != cudaSuccess) return cuda_fail(c, e, "join");
+    b.acc_stats = d_stats;
+    e = launch_split_fanout(c->split_variant, b, c->d_tx, d_active, n_active, base + off_recs, out, nullptr, nullptr,
+                            nullptr, c->stream);
+    c->launches += (n > 0) * 2;
+    if (e != cudaSuccess) return cuda_fail(c, e, "accuracy fan-out launch");
+    unsigned long long h[4] = {0, 0, 0, 0};
+    e = cudaMemcpyAsync(h, d_stats, sizeof h, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "accuracy fan-out");
+    double dd, dp;
+    memcpy(&dd, &h[0], sizeof dd);
+    memcpy(&dp, &h[1], sizeof dp);
+    *max_delay_err_s = dd;
+    *max_phase_err_rad = dp;
+    *n_fast = (int64_t)h[2];
+    *n_exact = (int64_t)h[3];
+    return LPK_OK;
+}
+
 lpk_status lpk_sync(lpk_ctx *c) {
     if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
     cudaError_t e = cudaStreamSynchronize(c->stream);

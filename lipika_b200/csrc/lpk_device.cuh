@@ -78,6 +78,8 @@ struct DevBand {
     unsigned long long *gate_stats;     // horizon gate counters (tested, skipped) or NULL
     uint32_t *unocc_words;              // split kernel: per active transmitter, set when any sample
                                         // has a non-zero antenna gain (NULL: not reported)
+    unsigned long long *acc_stats;      // split kernel in accuracy mode: (max delay error, max phase
+                                        // error) as double bits, (fast-path, exact-path) sample counts
     int32_t post_kind[3];
     float post_a[3], post_b[3];         // gain: g | nonlin: k | adc: fs, lsb
 };

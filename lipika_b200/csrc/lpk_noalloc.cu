@@ -5,14 +5,21 @@
 // allocator, a host that reserved the whole device up front for its own pool,
 // or an embedding where only pre-registered buffers may be touched. For them,
 // lpk_band_chunk_device_static does what lpk_band_chunk_device does — the
-// active list, the per-transmitter occlusion words and the receiver clock
-// walk (block totals, group sums, carries, the materialised walk) — in one file-scope
-// static device array instead of the context's growable scratch.
+// active list, the per-transmitter occlusion words, the receiver clock walk
+// (block totals, group sums, carries, the materialised walk) and, for a
+// split-solver band, the anchor records of the chunk's tiles — in one
+// file-scope static device array instead of the context's growable scratch,
+// running the same kernels on the same inputs (so the outputs are the same
+// bits).
 //
 // The array lives on every GPU that loads the library until the process exits.
 // Every call shares it and it keeps the last call's contents, so each call
 // clears what must start at zero; two calls that overlap on the GPU (on any
-// stream, from any context on the same device) race on it.
+// stream, from any context on the same device) race on it. Nothing of an
+// earlier call is trusted: the walk's block totals and carries are rebuilt
+// from master sample 0 on every call, so a call's walk work grows with the
+// chunk's master-sample offset (a chunk near the end of a band costs more
+// than one near its start).
 #include <cmath>
 #include <mutex>
 
@@ -29,7 +36,9 @@ constexpr size_t kOffTotals = kOffWords + sizeof(uint32_t) * kMaxActive;
 constexpr size_t kOffCarry = kOffTotals + sizeof(double) * kMaxWalkBlocks;
 constexpr size_t kOffGsum = kOffCarry + sizeof(double) * (kMaxWalkBlocks + 1);
 constexpr size_t kOffEps = (kOffGsum + sizeof(double) * (kMaxWalkBlocks / lpk::kGroupBlocks + 1) + 255) / 256 * 256;
-constexpr size_t kStaticBytes = kOffEps + sizeof(double) * kMaxWalkSpan;  // 10.0 MiB
+constexpr size_t kOffRecs = (kOffEps + sizeof(double) * kMaxWalkSpan + 255) / 256 * 256;
+constexpr size_t kMaxRecsBytes = size_t(12) << 20;  // split anchor records: 32,768 (tile, transmitter) pairs
+constexpr size_t kStaticBytes = kOffRecs + kMaxRecsBytes;  // 22.0 MiB
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
 
@@ -80,6 +89,10 @@ extern "C" lpk_status lpk_band_chunk_device_static(lpk_ctx *c, const lpk_band_de
             return fail(c, LPK_EINVAL, "chunk lies beyond 2^29 master-clock samples (static scratch limit)");
         sigma = band->clock_allan_1s / std::sqrt(band->clock_master_rate_hz);
     }
+    const bool split = use_split(band);
+    if (split && split_recs_bytes(c->split_variant, i0, n, n_active) > kMaxRecsBytes)
+        return fail(c, LPK_EINVAL, "chunk needs more split anchor records than the static scratch holds "
+                                   "(tiles x transmitters > 32768); use smaller chunks");
     cudaSetDevice(c->device);
     char *base = nullptr;
     if ((st = static_scratch(c, &base))) return st;
@@ -101,7 +114,13 @@ extern "C" lpk_status lpk_band_chunk_device_static(lpk_ctx *c, const lpk_band_de
         b.eps_k0 = kA;
         b.fm = band->clock_master_rate_hz;
     }
-    if (e == cudaSuccess) e = launch_band_reference(b, c->d_tx, d_active, n_active, (float2 *)d_out, d_words, c->stream);
+    if (e == cudaSuccess && split) {  // the split path of lpk_band_chunk_device, on one stream
+        b.unocc_words = b.has_antenna ? d_words : nullptr;
+        e = launch_band_split(c->split_variant, b, c->d_tx, d_active, n_active, base + kOffRecs, (float2 *)d_out,
+                              nullptr, nullptr, nullptr, c->stream);
+    } else if (e == cudaSuccess) {
+        e = launch_band_reference(b, c->d_tx, d_active, n_active, (float2 *)d_out, d_words, c->stream);
+    }
     if (e == cudaSuccess && d_unocc && n_active > 0)
         e = launch_or_flags(d_words, d_unocc, n_active, b.has_antenna ? 0 : (n > 0 ? 1 : 2), c->stream);
     if (e != cudaSuccess) return cuda_fail(c, e, "static-scratch fan-out");

@@ -30,7 +30,7 @@ k_split_anchor(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__
 }
 
 // One block per tile.
-template <int TILE, int THREADS, int MINB, bool DBG, bool UNOCC>
+template <int TILE, int THREADS, int MINB, bool DBG, bool UNOCC, bool ACC = false>
 __global__ void __launch_bounds__(THREADS, MINB)
 k_band_split(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__restrict__ active, int32_t n_active,
              int64_t t0, const AnchorRec *__restrict__ recs, const AnchorExt *__restrict__ exts,
@@ -43,8 +43,8 @@ k_band_split(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__re
     stage_tile(txs, active, n_active, recs + tile * n_active, stx, srec, true);
     __syncthreads();
     const int64_t first = (t0 + tile) * TILE - b.i0;  // chunk index of the tile's first sample
-    split_tile<TILE / THREADS, THREADS, DBG, UNOCC>(b, stx, srec, exts + tile * n_active, n_active, first, out,
-                                                    dbg_phase, dbg_temit, dbg_delay);
+    split_tile<TILE / THREADS, THREADS, DBG, UNOCC, ACC>(b, stx, srec, exts + tile * n_active, n_active, first, out,
+                                                         dbg_phase, dbg_temit, dbg_delay);
 }
 
 using SplitKernel = void (*)(const DevBand, const DevTx *, const int32_t *, int32_t, int64_t, const AnchorRec *,
@@ -52,12 +52,12 @@ using SplitKernel = void (*)(const DevBand, const DevTx *, const int32_t *, int3
 
 struct SplitShape {
     int tile, threads, minb;
-    SplitKernel fast, fast_unocc, dbg;
+    SplitKernel fast, fast_unocc, dbg, acc;  // acc: accuracy mode (DevBand::acc_stats)
 };
 
 #define LPK_SPLIT_ENTRY(I, T, N, M)                                                                              \
     {T, N, M, k_band_split<T, N, M, false, false>, k_band_split<T, N, M, false, true>,                           \
-     k_band_split<T, N, M, true, false>},
+     k_band_split<T, N, M, true, false>, k_band_split<T, N, M, false, false, true>},
 const SplitShape kShapes[kSplitVariants] = {LPK_SPLIT_VARIANTS(LPK_SPLIT_ENTRY)};
 #undef LPK_SPLIT_ENTRY
 
@@ -104,7 +104,7 @@ cudaError_t launch_split_fanout(int variant, const DevBand &b, const DevTx *d_tx
     AnchorRec *recs = (AnchorRec *)d_recs;
     AnchorExt *exts = (AnchorExt *)(recs + na);
     const size_t smem = (sizeof(DevTx) + sizeof(AnchorRec)) * (size_t)n_active;
-    SplitKernel kern = dbg_phase ? sh.dbg : (b.unocc_words ? sh.fast_unocc : sh.fast);
+    SplitKernel kern = b.acc_stats ? sh.acc : (dbg_phase ? sh.dbg : (b.unocc_words ? sh.fast_unocc : sh.fast));
     if (smem > 40 * 1024) {  // leaves room for the kernel's static shared arrays
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;

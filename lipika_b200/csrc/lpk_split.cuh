@@ -462,11 +462,16 @@ __device__ __forceinline__ void split_baseband(const DevTx &tx, const AnchorRec 
 // the samples inside the tile's fit range. DBG stores the diagnostics.
 // NK: grid nodes inside the tile (0: one piece per iterate; 1: two
 // pieces; kSplitNodes: up to four pieces, selected per sample).
-template <int K, bool DBG, int NK, int S, int THREADS>
+// ACC: every fast-path sample is also solved with the reference-exact FP64
+// arithmetic (the exact path's solve and phase) and the largest delay and
+// carrier-phase differences are kept in acc[0], acc[1]; acc[2] counts the
+// fast-path samples compared.
+template <int K, bool DBG, int NK, int S, int THREADS, bool ACC = false>
 __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, const AnchorExt *X, double epoch,
                                            const SampleCtx *sc,
                                            unsigned fit, float *ar, float *ai, unsigned &redo, int64_t first,
-                                           double *dbg_phase, double *dbg_temit, double *dbg_delay) {
+                                           double *dbg_phase, double *dbg_temit, double *dbg_delay,
+                                           const DevBand *acc_band = nullptr, double *acc = nullptr) {
     const double tu0 = R.tu0, k0 = R.k0;
     // A rounding error never exceeds half an ulp, so "|(|err| - half)| > tie"
     // (not within `tie` of a tie) is |err| < half - tie; half and tie are
@@ -535,6 +540,22 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
         const float amp = __fmaf_rn(amp1, __double2float_rn(d), amp0);
         const float vre = __fmaf_rn(bre, cs, __fmul_rn(-bim, sn)), vim = __fmaf_rn(bre, sn, __fmul_rn(bim, cs));
         ok &= (fit >> s) & 1u;
+        if constexpr (ACC) {
+            if (ok) {
+                const DevBand &b = *acc_band;
+                double te_ref, r_ref;
+                solve_reference(tx, tu, b.rx[0], b.rx[1], b.rx[2], epoch, 2, b.inv_c, te_ref, r_ref);
+                const double delay_ref = __dmul_rn(r_ref, b.inv_c);
+                const double tif = __dmul_rn(kTau, __dsub_rn(tx.carrier, b.lo));
+                const double ph_ref = __dadd_rn(__dmul_rn(tx.neg_tau_src, __dadd_rn(delay_ref, c.dl)),
+                                                __dmul_rn(tif, c.tl));
+                double dp = rr - remainder(ph_ref, kTau);
+                dp -= kTau * rint(dp * 0.15915494309189535);
+                acc[0] = fmax(acc[0], fabs(delay - delay_ref));
+                acc[1] = fmax(acc[1], fabs(dp));
+                acc[2] += 1.0;
+            }
+        }
         ar[s] = ok ? __fmaf_rn(amp, vre, ar[s]) : ar[s];
         ai[s] = ok ? __fmaf_rn(amp, vim, ai[s]) : ai[s];
         redo |= (unsigned)!ok << s;
@@ -555,13 +576,19 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
 // active-list order and the epilogue (AWGN, receiver chain) is applied.
 // UNOCC: report per-transmitter occlusion words (b.unocc_words; antenna
 // bands of the per-band path only).
-template <int S, int THREADS, bool DBG, bool UNOCC>
+// ACC: accuracy mode (see split_pass): the block's largest delay and phase
+// differences go to b.acc_stats[0..1] (atomic max on the bit patterns of
+// non-negative doubles), its fast-path and exact-path (sample, transmitter)
+// counts are added to b.acc_stats[2..3].
+template <int S, int THREADS, bool DBG, bool UNOCC, bool ACC = false>
 // xrec: the tile's AnchorExt records in global memory (index k per
 // transmitter), read only for tiles that cross more than one grid node.
 __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, const AnchorRec *srec,
                                            const AnchorExt *xrec, int n_active, int64_t first,
                                            float2 *__restrict__ out, double *dbg_phase, double *dbg_temit,
                                            double *dbg_delay) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    double acc_exact = 0.0;
     SampleCtx sc[S];
     float ar[S], ai[S];
     unsigned live = 0, fit = 0;
@@ -636,14 +663,15 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
 #define LPK_PASS(KIND)                                                                                           \
     do {                                                                                                         \
         if (nk == 0)                                                                                             \
-            split_pass<KIND, DBG, 0, S, THREADS>(T, R, xrec + k, b.epoch, sc, fit & live, ar, ai, redo, first, dbg_phase, \
-                                                 dbg_temit, dbg_delay);                                          \
+            split_pass<KIND, DBG, 0, S, THREADS, ACC>(T, R, xrec + k, b.epoch, sc, fit & live, ar, ai, redo, first,  \
+                                                      dbg_phase, dbg_temit, dbg_delay, &b, acc);                  \
         else if (nk == 1)                                                                                        \
-            split_pass<KIND, DBG, 1, S, THREADS>(T, R, xrec + k, b.epoch, sc, fit & live, ar, ai, redo, first, dbg_phase, \
-                                                 dbg_temit, dbg_delay);                                          \
+            split_pass<KIND, DBG, 1, S, THREADS, ACC>(T, R, xrec + k, b.epoch, sc, fit & live, ar, ai, redo, first,  \
+                                                      dbg_phase, dbg_temit, dbg_delay, &b, acc);                  \
         else                                                                                                     \
-            split_pass<KIND, DBG, kSplitNodes, S, THREADS>(T, R, xrec + k, b.epoch, sc, fit & live, ar, ai, redo, first,  \
-                                                           dbg_phase, dbg_temit, dbg_delay);                     \
+            split_pass<KIND, DBG, kSplitNodes, S, THREADS, ACC>(T, R, xrec + k, b.epoch, sc, fit & live, ar, ai,     \
+                                                                redo, first, dbg_phase, dbg_temit, dbg_delay, &b,  \
+                                                                acc);                                             \
     } while (0)
             switch (pass_kind(T, R)) {
             case kPassCa: LPK_PASS(kPassCa); break;
@@ -660,6 +688,7 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
                     atomicOr(b.unocc_words + k, 1u);
             }
         }
+        if constexpr (ACC) acc_exact += (double)__popc(redo & (gate_off ? outside : live));
         if (redo == 0) continue;
 #pragma unroll
         for (int s = 0; s < S; ++s) {  // the exact path: rare samples, or whole exact tiles
@@ -683,6 +712,20 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
                 dbg_temit[j] = te;
                 dbg_delay[j] = rg * b.inv_c;
             }
+        }
+    }
+    if constexpr (ACC) {
+        for (int off = 16; off > 0; off >>= 1) {
+            acc[0] = fmax(acc[0], __shfl_xor_sync(0xffffffffu, acc[0], off));
+            acc[1] = fmax(acc[1], __shfl_xor_sync(0xffffffffu, acc[1], off));
+            acc[2] += __shfl_xor_sync(0xffffffffu, acc[2], off);
+            acc_exact += __shfl_xor_sync(0xffffffffu, acc_exact, off);
+        }
+        if ((threadIdx.x & 31) == 0 && b.acc_stats) {
+            atomicMax(b.acc_stats + 0, (unsigned long long)__double_as_longlong(acc[0]));
+            atomicMax(b.acc_stats + 1, (unsigned long long)__double_as_longlong(acc[1]));
+            atomicAdd(b.acc_stats + 2, (unsigned long long)acc[2]);
+            atomicAdd(b.acc_stats + 3, (unsigned long long)acc_exact);
         }
     }
 #pragma unroll

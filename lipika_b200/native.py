@@ -134,6 +134,8 @@ SIGNATURES = {
     "lpk_band_chunk_device": (C.c_int32, [_VP, C.POINTER(BandDesc), _I32, C.c_int32, C.c_int64, C.c_int64,
                                           _VP, _VP, _VP, _VP]),
     "lpk_sync": (C.c_int32, [_VP]),
+    "lpk_split_accuracy": (C.c_int32, [_VP, C.POINTER(BandDesc), _I32, C.c_int32, C.c_int64, C.c_int64, _VP, _VP,
+                                       _D, _D, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "lpk_band_chunk_device_static": (C.c_int32, [_VP, C.POINTER(BandDesc), _I32, C.c_int32, C.c_int64, C.c_int64,
                                                  _VP, _VP, _VP, _VP]),
     "lpk_solve_emission_times": (C.c_int32, [_VP, C.c_int32, _D, _D, C.c_int64, C.c_double, C.c_int32, _D, _D]),

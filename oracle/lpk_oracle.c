@@ -14,6 +14,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <pthread.h>
+#include <time.h>
 
 #define TAU 6.283185307179586476925286766559
 static const double SPEED_OF_LIGHT_M_S = 299792458.0;      /* src/lib.rs:53 */
@@ -706,6 +707,31 @@ void orc_solve_converged(const orc_traj *src, const double *obs, const double *t
 }
 
 /* accumulate_reporting_occlusion, src/channel/mod.rs:164-271 */
+/* The mix loop of accumulate_reporting_occlusion, src/channel/mod.rs:236-268:
+ * phase in f64, f64 sin/cos, f32 amplitude and complex MAC into acc. */
+static void mix_into(float *acc, double src_carrier, const double *ranges, const float *bb, const float *gg,
+                     const double *t_local, const double *delta_t, int64_t n, double lo_hz, double tx_power_w) {
+    double wavelength_m = SPEED_OF_LIGHT_M_S / src_carrier;
+    double tx_amplitude_v = sqrt(tx_power_w);
+    double neg_tau_src = -TAU * src_carrier;
+    double tau_if = TAU * (src_carrier - lo_hz);
+    double amp_factor = (wavelength_m / (2.0 * TAU)) * tx_amplitude_v;
+    double inv_c = 1.0 / SPEED_OF_LIGHT_M_S;
+    for (int64_t i = 0; i < n; i++) {
+        float g = gg ? gg[i] : 1.0f;
+        if (g == 0.0f) continue;
+        double r = ranges[i];
+        double delay = r * inv_c;
+        double phase = neg_tau_src * (delay + delta_t[i]) + tau_if * t_local[i];
+        double sp = sin(phase), cp = cos(phase);
+        float amplitude = (float)(amp_factor / r) * g;
+        float br = bb[2 * i], bi = bb[2 * i + 1];
+        float cpf = (float)cp, spf = (float)sp;
+        acc[2 * i] = acc[2 * i] + amplitude * (br * cpf - bi * spf);
+        acc[2 * i + 1] = acc[2 * i + 1] + amplitude * (br * spf + bi * cpf);
+    }
+}
+
 int orc_accumulate(float *acc, const orc_signal *sig, const orc_traj *traj, const double *obs,
                    const double *t_local, const double *t_utc, const double *delta_t, int64_t n,
                    double lo_hz, double tx_power_w, double epoch, int iterations,
@@ -736,26 +762,7 @@ int orc_accumulate(float *acc, const orc_signal *sig, const orc_traj *traj, cons
         free(abs_emit);
         free(src);
     }
-    double src_carrier = sig->carrier_hz;
-    double wavelength_m = SPEED_OF_LIGHT_M_S / src_carrier;
-    double tx_amplitude_v = sqrt(tx_power_w);
-    double neg_tau_src = -TAU * src_carrier;
-    double tau_if = TAU * (src_carrier - lo_hz);
-    double amp_factor = (wavelength_m / (2.0 * TAU)) * tx_amplitude_v;
-    double inv_c = 1.0 / SPEED_OF_LIGHT_M_S;
-    for (int64_t i = 0; i < n; i++) {
-        float g = gg ? gg[i] : 1.0f;
-        if (g == 0.0f) continue;
-        double r = ranges[i];
-        double delay = r * inv_c;
-        double phase = neg_tau_src * (delay + delta_t[i]) + tau_if * t_local[i];
-        double sp = sin(phase), cp = cos(phase);
-        float amplitude = (float)(amp_factor / r) * g;
-        float br = bb[2 * i], bi = bb[2 * i + 1];
-        float cpf = (float)cp, spf = (float)sp;
-        acc[2 * i] = acc[2 * i] + amplitude * (br * cpf - bi * spf);
-        acc[2 * i + 1] = acc[2 * i + 1] + amplitude * (br * spf + bi * cpf);
-    }
+    mix_into(acc, sig->carrier_hz, ranges, bb, gg, t_local, delta_t, n, lo_hz, tx_power_w);
     free(t_emit); free(ranges); free(bb); free(gg);
     return unoccluded;
 }
@@ -951,6 +958,12 @@ orc_clock *orc_clock_new(const lpk_clock_cfg *spec, double start_epoch, double m
 }
 /* ClockStream::advance_to, src/clock/mod.rs:299-307 */
 static void clock_advance_to(orc_clock *c, int64_t k) {
+    /* without a walk every step keeps eps at 0: jump the frontier (exact) */
+    if (!c->has_walk && c->frontier < k) {
+        c->eps_lo = c->eps_hi;
+        c->frontier = k;
+        return;
+    }
     while (c->frontier < k) {
         c->eps_lo = c->eps_hi;
         if (c->has_walk) c->eps_hi += 0.0 + c->step_std * orc_std_normal(&c->rng);
@@ -1129,11 +1142,26 @@ static void *fan_worker(void *arg) {
 int orc_generate_band(const orc_scene *s, int r_idx, int b_idx, uint64_t seed_base, int work_idx,
                       int64_t chunk_samples, int n_threads, int noise_mode, int64_t sample_limit,
                       float *out, double *out_delta, uint8_t *unoccluded) {
+    return orc_generate_band_window(s, r_idx, b_idx, seed_base, work_idx, chunk_samples, n_threads, noise_mode, 0,
+                                    sample_limit, out, out_delta, unoccluded);
+}
+
+/* The same loop over band samples [sample_start, sample_start + sample_limit)
+ * only (chunk boundaries at sample_start + k chunk_samples): the window a
+ * render_window-style caller asks for (src/pipeline.rs:746-794). The
+ * sequential AWGN stream cannot start mid-band, so a window that does not
+ * start at 0 takes NOISE_NONE or NOISE_COUNTER only. */
+int orc_generate_band_window(const orc_scene *s, int r_idx, int b_idx, uint64_t seed_base, int work_idx,
+                             int64_t chunk_samples, int n_threads, int noise_mode, int64_t sample_start,
+                             int64_t sample_limit, float *out, double *out_delta, uint8_t *unoccluded) {
     const orc_rx *rx = &s->rx[r_idx];
     const lpk_band_cfg *band = &rx->bands[b_idx];
     double epoch = s->cfg.epoch_unix;
     double fs = band->sample_rate_hz;
-    int64_t n = orc_band_n_samples(s, r_idx, b_idx);
+    int64_t n_band = orc_band_n_samples(s, r_idx, b_idx);
+    if (sample_start < 0 || sample_start > n_band) return -2;
+    if (sample_start > 0 && noise_mode == ORC_NOISE_SEQUENTIAL) return -3;
+    int64_t n = n_band - sample_start;
     if (sample_limit >= 0 && sample_limit < n) n = sample_limit;
     double lo = band->lo_carrier_hz;
     double master = 0.0;
@@ -1163,7 +1191,7 @@ int orc_generate_band(const orc_scene *s, int r_idx, int b_idx, uint64_t seed_ba
     for (int64_t i0 = 0; i0 < n; i0 += chunk_samples) {
         int64_t i1 = i0 + chunk_samples < n ? i0 + chunk_samples : n;
         int64_t clen = i1 - i0;
-        for (int64_t j = 0; j < clen; j++) t_local[j] = (double)(i0 + j) / fs;
+        for (int64_t j = 0; j < clen; j++) t_local[j] = (double)(sample_start + i0 + j) / fs;
         for (int64_t j = 0; j < clen; j++) delta[j] = orc_clock_delta_t_at(clock, t_local[j]);
         for (int64_t j = 0; j < clen; j++) t_utc[j] = t_local[j] - delta[j];
         for (int64_t j = 0; j < clen; j++) t_abs[j] = epoch + t_utc[j];
@@ -1195,7 +1223,7 @@ int orc_generate_band(const orc_scene *s, int r_idx, int b_idx, uint64_t seed_ba
         } else if (noise_mode == ORC_NOISE_COUNTER && noise_power > 0.0) {
             for (int64_t j = 0; j < clen; j++) {
                 float zr, zi;
-                orc_noise_pair(nseed, i0 + j, &zr, &zi);
+                orc_noise_pair(nseed, sample_start + i0 + j, &zr, &zi);
                 acc[2 * j] += noise_std * zr;
                 acc[2 * j + 1] += noise_std * zi;
             }
@@ -1205,5 +1233,95 @@ int orc_generate_band(const orc_scene *s, int r_idx, int b_idx, uint64_t seed_ba
     }
     free(t_local); free(delta); free(t_utc); free(t_abs); free(rxp); free(contrib); free(unocc_chunk);
     orc_clock_free(clock);
+    return 0;
+}
+
+/* Single-thread cost of the sections of generate_band's loop
+ * (src/pipeline.rs:911-983) on the first n samples of band (r_idx, b_idx),
+ * in one chunk, with the horizon gate off and no antenna: ns_out[0] clock
+ * offsets (per band sample), [1] receiver positions (per band sample),
+ * [2] emission solves, [3] baseband, [4] mix (phase, f64 sin/cos, f32 MAC)
+ * (each per tx-rx sample), [5] fixed-order sum (per band sample), [6] AWGN
+ * (per band sample), [7] the largest |carrier phase| argument handed to
+ * sin/cos (rad). Test infrastructure: times the restatement, not the
+ * reference binary. */
+static double now_ns(void) {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return 1e9 * (double)ts.tv_sec + (double)ts.tv_nsec;
+}
+int orc_profile_sections(const orc_scene *s, int r_idx, int b_idx, uint64_t seed_base, int64_t n, double *ns_out) {
+    const orc_rx *rx = &s->rx[r_idx];
+    const lpk_band_cfg *band = &rx->bands[b_idx];
+    int64_t nb = orc_band_n_samples(s, r_idx, b_idx);
+    if (n > nb) n = nb;
+    if (n <= 0) return -1;
+    double fs = band->sample_rate_hz, epoch = s->cfg.epoch_unix, lo = band->lo_carrier_hz;
+    double master = 0.0;
+    for (int b = 0; b < rx->n_bands; b++) master = fmax(master, rx->bands[b].sample_rate_hz);
+    int32_t active[256];
+    int na = orc_band_active(s, r_idx, b_idx, active, 256);
+    if (na > 256) return -1;
+    double *t_local = malloc(sizeof(double) * (size_t)n), *delta = malloc(sizeof(double) * (size_t)n);
+    double *t_utc = malloc(sizeof(double) * (size_t)n), *t_abs = malloc(sizeof(double) * (size_t)n);
+    double *rxp = malloc(sizeof(double) * 3 * (size_t)n), *te = malloc(sizeof(double) * (size_t)n);
+    double *rg = malloc(sizeof(double) * (size_t)n);
+    float *bb = malloc(sizeof(float) * 2 * (size_t)n);
+    float *contrib = calloc(2 * (size_t)n * (size_t)(na ? na : 1), sizeof(float));
+    float *acc = malloc(sizeof(float) * 2 * (size_t)n);
+    for (int i = 0; i < 8; i++) ns_out[i] = 0.0;
+    double t0 = now_ns();
+    orc_clock *clock = orc_clock_new(&rx->clock, 0.0, master, orc_clock_seed(seed_base, (uint64_t)r_idx));
+    for (int64_t j = 0; j < n; j++) t_local[j] = (double)j / fs;
+    for (int64_t j = 0; j < n; j++) delta[j] = orc_clock_delta_t_at(clock, t_local[j]);
+    double t1 = now_ns();
+    for (int64_t j = 0; j < n; j++) t_utc[j] = t_local[j] - delta[j];
+    for (int64_t j = 0; j < n; j++) t_abs[j] = epoch + t_utc[j];
+    orc_traj_position_batch(&rx->traj, t_abs, n, rxp);
+    double t2 = now_ns();
+    ns_out[0] = (t1 - t0) / (double)n;
+    ns_out[1] = (t2 - t1) / (double)n;
+    double solve = 0.0, base = 0.0, mix = 0.0, big = 0.0;
+    for (int k = 0; k < na; k++) {
+        const orc_tx *tx = &s->tx[active[k]];
+        double a = now_ns();
+        orc_solve_emission_times(&tx->traj, rxp, t_utc, n, epoch, NEWTON_ITERATIONS, te, rg);
+        double b = now_ns();
+        orc_signal_eval(&tx->sig, te, n, bb);
+        double c = now_ns();
+        mix_into(contrib + (size_t)k * 2 * (size_t)n, tx->sig.carrier_hz, rg, bb, NULL, t_local, delta, n, lo,
+                 tx->power_w);
+        double d = now_ns();
+        solve += b - a;
+        base += c - b;
+        mix += d - c;
+        double nts = -TAU * tx->sig.carrier_hz, tif = TAU * (tx->sig.carrier_hz - lo);
+        for (int64_t j = 0; j < n; j += 997) big = fmax(big, fabs(nts * (rg[j] / SPEED_OF_LIGHT_M_S + delta[j]) +
+                                                              tif * t_local[j]));
+    }
+    double t3 = now_ns();
+    for (int64_t j = 0; j < 2 * n; j++) acc[j] = 0.0f;
+    for (int k = 0; k < na; k++) {
+        const float *c = contrib + (size_t)k * 2 * (size_t)n;
+        for (int64_t j = 0; j < 2 * n; j++) acc[j] = acc[j] + c[j];
+    }
+    double t4 = now_ns();
+    orc_xoshiro noise_rng;
+    orc_xoshiro_seed(&noise_rng, 12345);
+    for (int64_t j = 0; j < n; j++) {
+        acc[2 * j] += 0.0f + 1e-7f * (float)orc_std_normal(&noise_rng);
+        acc[2 * j + 1] += 0.0f + 1e-7f * (float)orc_std_normal(&noise_rng);
+    }
+    double t5 = now_ns();
+    double ntx = (double)n * (double)(na ? na : 1);
+    ns_out[2] = solve / ntx;
+    ns_out[3] = base / ntx;
+    ns_out[4] = mix / ntx;
+    ns_out[5] = (t4 - t3) / (double)n;
+    ns_out[6] = (t5 - t4) / (double)n;
+    ns_out[7] = big;
+    orc_clock_free(clock);
+    free(t_local); free(delta); free(t_utc); free(t_abs); free(rxp); free(te); free(rg); free(bb); free(contrib);
+    free(acc);
     return 0;
 }

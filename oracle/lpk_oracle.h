@@ -169,6 +169,12 @@ int orc_generate_band(const orc_scene *s, int r_idx, int b_idx, uint64_t seed_ba
                       int64_t chunk_samples, int n_threads, int noise_mode,
                       int64_t sample_limit, float *out_iq2n, double *out_delta,
                       uint8_t *unoccluded);
+int orc_generate_band_window(const orc_scene *s, int r_idx, int b_idx, uint64_t seed_base, int work_idx,
+                             int64_t chunk_samples, int n_threads, int noise_mode, int64_t sample_start,
+                             int64_t sample_limit, float *out, double *out_delta, uint8_t *unoccluded);
+/* Single-thread cost of each section of the loop on the first n samples of
+ * a band (ns per band or tx-rx sample; see lpk_oracle.c). */
+int orc_profile_sections(const orc_scene *s, int r_idx, int b_idx, uint64_t seed_base, int64_t n, double *ns_out);
 
 #ifdef __cplusplus
 }

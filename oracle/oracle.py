@@ -130,6 +130,10 @@ def lib():
             "orc_scene_tx_power_w": (C.c_double, [C.c_void_p, C.c_int]),
             "orc_generate_band": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int64, C.c_int,
                                             C.c_int, C.c_int64, _F, _D, C.POINTER(C.c_uint8)]),
+            "orc_profile_sections": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_uint64, C.c_int64, _D]),
+            "orc_generate_band_window": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_uint64, C.c_int, C.c_int64,
+                                                   C.c_int, C.c_int, C.c_int64, C.c_int64, _F, _D,
+                                                   C.POINTER(C.c_uint8)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -223,6 +227,30 @@ class Scene:
         if want_delta:
             res["delta"] = delta[:n]
         return res
+
+    def generate_window(self, r, b, seed, work_idx, start, n, chunk=1 << 20, threads=1, noise=NOISE_NONE):
+        """Band samples [start, start + n) through the same loop (chunks
+        begin at `start`); noise NONE or COUNTER."""
+        n = max(0, min(n, self.n_samples(r, b) - start))
+        out = np.zeros(2 * max(n, 1), dtype=np.float32)
+        na = len(self.active(r, b))
+        unocc = (C.c_uint8 * max(na, 1))()
+        rc = lib().orc_generate_band_window(self.h, r, b, seed, work_idx, chunk, threads, noise, start, n,
+                                            fptr(out), None, unocc)
+        if rc:
+            raise RuntimeError(f"oracle generate_band_window failed ({rc})")
+        return out[: 2 * n].view(np.complex64)
+
+    def profile_sections(self, r, b, seed, n):
+        """Single-thread ns per sample of each section of the loop on the
+        first n samples of band (r, b): clock, rx, solve, baseband, mix,
+        sum, awgn, and the largest carrier-phase argument (rad)."""
+        out = np.zeros(8)
+        if lib().orc_profile_sections(self.h, r, b, seed, n, dptr(out)):
+            raise RuntimeError("oracle profile failed")
+        keys = ("clock_ns_per_band_sample", "rx_ns_per_band_sample", "solve_ns_per_txrx", "baseband_ns_per_txrx",
+                "mix_ns_per_txrx", "sum_ns_per_band_sample", "awgn_ns_per_band_sample", "max_phase_rad")
+        return dict(zip(keys, out.tolist()))
 
     def run(self, seed, chunk=1 << 20, threads=1, noise=NOISE_NONE):
         """run_scene (src/pipeline.rs:443-485): every (rx, band) in order."""

@@ -4,8 +4,10 @@ A host that renders from a real-time thread, or one that owns the whole
 device through its own pool, cannot let the library call cudaMalloc while it
 renders. The static entry point keeps its working memory in one file-scope
 device array instead; these checks call it through the C ABI and compare it
-with lpk_band_chunk_device, chunk after chunk (the array keeps the previous
-call's contents, so the second call shows nothing stale leaks through).
+with lpk_band_chunk_device, chunk after chunk, for both solvers and with an
+antenna (the array keeps the previous call's contents, so the second call
+shows nothing stale leaks through), and time the walk rebuild it does on
+every call.
 This file is collected last on purpose.
 """
 import ctypes as C
@@ -27,18 +29,15 @@ def _run(entry, ctx, d, act, na, i0, n, out, flags):
     N.check(N.lib().lpk_sync(ctx.h), ctx.h)
 
 
-def test_static_scratch_matches_allocating_entry_point_two_calls():
+def _compare_two_calls(ctx, prep, d, r, b, n, starts, expect_flags=None):
+    """Both entry points on the same chunks, one call after the other; the
+    static one must give the allocating one's bits (same kernels, same
+    inputs) and never anything stale from the call before."""
     import torch
-    ctx = N.Context(0)
-    prep = P.Prepared(scenes.config_c1(duration_s=4.0), ctx)
     L = N.lib()
-    r, b = 0, 1  # the 2.048 MS/s band, six C/A transmitters
-    d = prep.band_desc(r, b, 2026, 1)
-    d.clock_mode = N.LPK_CLOCK_DEVICE_WALK  # the path that needs scratch for the walk
     act_list = prep.active(r, b)
     act = (C.c_int32 * len(act_list))(*act_list)
-    n = 500_000
-    for i0 in (3_000_000, 123_457):  # two calls in a row, the second earlier in the band
+    for i0 in starts:
         ref = torch.zeros(2 * n, dtype=torch.float32, device="cuda")
         got = torch.full((2 * n,), float("nan"), dtype=torch.float32, device="cuda")
         fr = torch.zeros(len(act_list), dtype=torch.uint8, device="cuda")
@@ -51,7 +50,73 @@ def test_static_scratch_matches_allocating_entry_point_two_calls():
         scale = float(np.max(np.abs(a)))
         assert scale > 0
         assert float(np.max(np.abs(g.astype(np.complex128) - a))) <= IQ_RTOL * scale
-        assert fr.cpu().tolist() == fg.cpu().tolist() == [1] * len(act_list)
+        assert np.array_equal(a, g), (i0, d.solver)
+        assert fr.cpu().tolist() == fg.cpu().tolist()
+        if expect_flags is not None:
+            assert fg.cpu().tolist() == expect_flags(len(act_list))
+
+
+def test_static_scratch_matches_allocating_entry_point_two_calls():
+    ctx = N.Context(0)
+    prep = P.Prepared(scenes.config_c1(duration_s=4.0), ctx)
+    r, b = 0, 1  # the 2.048 MS/s band, six C/A transmitters
+    d = prep.band_desc(r, b, 2026, 1)
+    d.clock_mode = N.LPK_CLOCK_DEVICE_WALK  # the path that needs scratch for the walk
+    for solver in (N.LPK_SOLVER_REFERENCE, N.LPK_SOLVER_SPLIT):
+        d.solver = solver
+        # two calls in a row, the second earlier in the band
+        _compare_two_calls(ctx, prep, d, r, b, 500_000, (3_000_000, 123_457), lambda k: [1] * k)
+    prep.close()
+    ctx.close()
+
+
+def test_static_scratch_antenna_band_both_solvers():
+    """A band with an antenna (per-transmitter occlusion flags from the
+    kernel) over a 64-transmitter sky, both solvers."""
+    from lipika_b200 import config as cfg
+    ctx = N.Context(0)
+    sc = scenes.config_c4(duration_s=2.0, n_rx=1, noise=False)
+    sc.receivers[0].bands[0].frontend = cfg.Frontend(
+        antenna={"peak_dbi": 3.9, "horizon_dbi": -3.0, "fb_db": 8.5, "cutoff_deg": 10.0})
+    prep = P.Prepared(sc, ctx)
+    d = prep.band_desc(0, 0, 2026, 0)
+    d.clock_mode = N.LPK_CLOCK_DEVICE_WALK
+    assert d.has_antenna
+    for solver in (N.LPK_SOLVER_REFERENCE, N.LPK_SOLVER_SPLIT):
+        d.solver = solver
+        _compare_two_calls(ctx, prep, d, 0, 0, 200_000, (1_000_000, 0))
+    prep.close()
+    ctx.close()
+
+
+def test_static_scratch_walk_cost_grows_with_offset():
+    """Every call rebuilds the walk from master sample 0: one chunk near the
+    end of a 120 s band costs more than the same chunk at its start."""
+    import torch
+    ctx = N.Context(0)
+    prep = P.Prepared(scenes.config_c1(duration_s=120.0), ctx)
+    L = N.lib()
+    d = prep.band_desc(0, 1, 2026, 1)
+    d.clock_mode = N.LPK_CLOCK_DEVICE_WALK
+    d.solver = N.LPK_SOLVER_SPLIT
+    act_list = prep.active(0, 1)
+    act = (C.c_int32 * len(act_list))(*act_list)
+    n = 1 << 19
+    out = torch.zeros(2 * n, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.ExternalStream(L.lpk_ctx_stream(ctx.h))
+    ms = {}
+    for i0 in (0, 118 * 2_048_000):
+        for rep in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            N.check(L.lpk_band_chunk_device_static(ctx.h, C.byref(d), act, len(act_list), i0, n, None, None,
+                                                   out.data_ptr(), None), ctx.h)
+            e1.record(stream)
+            e1.synchronize()
+            ms[i0] = e0.elapsed_time(e1)
+    print(f"static entry point, 2^19 samples x 6 transmitters: {ms[0]:.3f} ms at 0 s, "
+          f"{ms[118 * 2_048_000]:.3f} ms at 118 s")
+    assert ms[118 * 2_048_000] > ms[0]
     prep.close()
     ctx.close()
 
