@@ -50,6 +50,8 @@ typedef struct lpk_cf32 { float re, im; } lpk_cf32;
 /* Create a context bound to CUDA device `device` (own stream + buffers).
  * Replaces: Backend::Cpu selection, src/backend/mod.rs:16-18. */
 lpk_status lpk_ctx_create(lpk_ctx **out, int32_t device);
+/* Destroy every scene, batch and network made on a context before the
+ * context: their handles refer to it. */
 void lpk_ctx_destroy(lpk_ctx *ctx);
 /* Message of the last failed call on this context ("" if none). */
 const char *lpk_last_error(const lpk_ctx *ctx);
@@ -152,7 +154,16 @@ lpk_status lpk_kepler_tables(lpk_ctx *ctx, const lpk_kepler_orbit *orbits, int32
 enum { LPK_CLOCK_HOST = 0, LPK_CLOCK_DETERMINISTIC = 1, LPK_CLOCK_DEVICE_WALK = 2 };
 enum { LPK_RX_STATIONARY = 0, LPK_RX_PER_SAMPLE = 1 };
 enum { LPK_POST_GAIN = 0, LPK_POST_NONLINEARITY = 1, LPK_POST_ADC = 2 };
-enum { LPK_SOLVER_REFERENCE = 0, LPK_SOLVER_SPLIT = 1 };
+/* Fan-out solvers: REFERENCE, the reference's per-sample f64 arithmetic in
+ * its order (bit-exact emission times, indices and ADC codes); SPLIT, the
+ * split-precision fan-out (FP64 anchors per tile, FP32 mix; delay within
+ * 1 ps, carrier phase within 1e-6 rad, IQ within 1e-5 of REFERENCE);
+ * FP64_TUNED, the same two iterations all in FP64 with the shortcuts a tuned
+ * FP64 kernel takes (table lerp scaled by 1/dt, carrier and CW phases
+ * reduced modulo 2π before one FP64 sincos, f32 amplitude division; within
+ * the IQ tolerance of REFERENCE; per-band entry points only, the batch runs
+ * REFERENCE for it). */
+enum { LPK_SOLVER_REFERENCE = 0, LPK_SOLVER_SPLIT = 1, LPK_SOLVER_FP64_TUNED = 2 };
 
 typedef struct lpk_post_op {
     int32_t kind;               /* LPK_POST_* */
@@ -366,53 +377,81 @@ lpk_status lpk_batch_autotune(lpk_batch *b, int64_t round, int32_t reps, double 
  * src/channel/mod.rs:355-383, runs four iterations), on the same
  * trajectory model (lerp table, linearised Sagnac), from one of three
  * starts: the reference's t - 70 ms (LAG), the range at the reception time
- * R(t)/c (GEOMETRIC), or R(t)/c plus the light-time correction predicted by
- * a trained lpk_mlp (LEARNED). A start that does not converge within
+ * from the trajectory table R(t)/c (GEOMETRIC), or the scene's surrogate
+ * (LEARNED, see lpk_mlp below). A start that does not converge within
  * max_iter falls back to LAG; iters[i] counts every map evaluation (-1 if
  * even the fallback did not converge) and start_err[i] (may be NULL) is
  * |start - converged delay| in seconds. No reference counterpart. */
 enum { LPK_START_LAG = 0, LPK_START_GEOMETRIC = 1, LPK_START_LEARNED = 2 };
 enum { LPK_ITER_FIXED_POINT = 0, LPK_ITER_NEWTON = 1 };
-#define LPK_MLP_N_FEATURES 8
-#define LPK_MLP_N_PARAMS 4801  /* W1 64x8, b1 64, W2 64x64, b2 64, w3 64, b3 (FP32, row-major) */
-#define LPK_MLP_N_NORM 18      /* feature means (8), feature stds (8), target mean, target std (µs) */
+#define LPK_MLP_N_FEATURES 16
+#define LPK_MLP_N_PARAMS 9473  /* W1 64x16, b1 64, W2 64x64, b2 64, W3 64x64, b3 64, w4 64, b4 (FP32, row-major) */
+#define LPK_MLP_N_NORM 34      /* feature means (16), feature stds (16), target mean, target std (µs) */
 typedef struct lpk_mlp lpk_mlp;
 
 lpk_status lpk_solve_converged(lpk_ctx *ctx, int32_t tx, const double *rx_ecef, double epoch,
                                const double *t_rel_utc, int64_t n, double tol_s, int32_t max_iter,
                                int32_t scheme, int32_t start, const lpk_mlp *mlp, double *t_emit,
                                int32_t *iters, float *start_err);
-/* The network's raw input features at the reception times: line-of-sight
- * unit vector (3), R/c, range rate / c, v_x / c, v_y / c, Sagnac rate of
- * the line of sight (n x 8, host memory). */
-lpk_status lpk_solve_features(lpk_ctx *ctx, int32_t tx, const double *rx_ecef, double epoch,
-                              const double *t_rel_utc, int64_t n, float *features);
-/* A tanh MLP 8 -> 64 -> 64 -> 1 whose output, de-normalised, is the
- * light-time correction tau - R/c in microseconds. Glorot-uniform initial
- * weights from `seed`. Forward, backward and the weight gradients run on
- * the tensor cores with BF16 operands and FP32 accumulation (inference and
- * the weight gradients on tcgen05 with a TMEM accumulator, training's
- * forward and backward activations as register mma.sync tiles); Adam
- * updates FP32 master weights. */
+/* The same over many (transmitter, receiver) pairs at once: sample i solves
+ * transmitter tx[i] for receiver rx_ecef[3 rx[i] .. 3 rx[i] + 2] (n_rx
+ * receivers). device_ms (may be NULL) receives the device time of the
+ * call's kernels (features, network and solve; CUDA events on the
+ * context's stream, host copies excluded). Host memory. */
+lpk_status lpk_solve_converged_scene(lpk_ctx *ctx, const int32_t *tx, const int32_t *rx, const double *rx_ecef,
+                                     int32_t n_rx, double epoch, const double *t_rel_utc, int64_t n, double tol_s,
+                                     int32_t max_iter, int32_t scheme, int32_t start, const lpk_mlp *mlp,
+                                     double *t_emit, int32_t *iters, float *start_err, double *device_ms);
+/* The scene's surrogate of the emission delay: a function of a
+ * transmitter's circular-orbit elements (lpk_kepler_orbit), a receiver's
+ * ECEF position and the reception time t (scene-epoch relative) alone. An
+ * analytic layer turns them into 16 features (the elements a, inclination,
+ * RAAN and true anomaly at epoch; the receiver's x, y, z; t; and, from the
+ * orbit at t: the line-of-sight unit vector, R/c, range rate / c, v_x / c,
+ * v_y / c and the Sagnac rate of the line of sight); a tanh MLP
+ * 16 -> 64 -> 64 -> 64 -> 1 predicts from them, normalised, the light-time
+ * correction tau - R/c (µs); the learned start is R/c plus that correction.
+ * One network covers every (transmitter, receiver) pair of a scene.
+ * Glorot-uniform initial weights from `seed`. Inference runs on tcgen05
+ * tensor cores (BF16 operands, FP32 accumulator in TMEM); training's
+ * products are BF16 mma.sync tiles with FP32 accumulation; Adam updates
+ * FP32 master weights. */
 lpk_status lpk_mlp_create(lpk_ctx *ctx, uint64_t seed, lpk_mlp **out);
 void lpk_mlp_destroy(lpk_mlp *mlp);
 lpk_status lpk_mlp_get_params(const lpk_mlp *mlp, float *params, float *norm);
 lpk_status lpk_mlp_set_params(lpk_mlp *mlp, const float *params, const float *norm);
+/* The network's transmitters: tx[k] (uploaded scene indices, moving) with
+ * circular orbit orbits[k]. lpk_mlp_fit sets them; a network restored with
+ * lpk_mlp_set_params needs them before it can serve a learned start. */
+lpk_status lpk_mlp_set_orbits(lpk_mlp *mlp, const int32_t *tx, const lpk_kepler_orbit *orbits, int32_t n_tx);
 /* y = MLP(x) on n rows of normalised features (host memory). */
 lpk_status lpk_mlp_forward(lpk_mlp *mlp, const float *x, int64_t n, float *y);
 /* Mean squared error over n rows and its gradient (LPK_MLP_N_PARAMS floats,
  * the parameter layout above); host memory. */
 lpk_status lpk_mlp_loss_grad(lpk_mlp *mlp, const float *x, const float *t, int64_t n, double *loss,
                              float *grad);
-/* Train on n_train reception times uniform in [t0, t1) of transmitter tx
- * seen from rx_ecef: the converged Newton solver (geometric start) produces
- * the targets on the GPU, the normalisation comes from the training set,
- * then `steps` Adam steps on batches of `batch` rows with a cosine-decayed
- * learning rate. loss_curve (may be NULL) receives each step's batch MSE in
- * normalised units. */
-lpk_status lpk_mlp_fit(lpk_mlp *mlp, int32_t tx, const double *rx_ecef, double epoch, double t0, double t1,
-                       int64_t n_train, int32_t steps, int32_t batch, float lr, uint64_t seed,
-                       float *loss_curve);
+/* Train on n_train (transmitter, receiver, reception time) triples: orbit k
+ * and receiver j drawn uniformly (tx[k], orbits[k]; rx_ecef holds n_rx
+ * positions), t uniform in [t0, t1). The converged Newton solver (started
+ * at the orbit's R/c) produces the targets on the GPU, the normalisation
+ * comes from the first 2^21 rows of the training set, then `steps` Adam
+ * steps on batches of `batch` rows with a cosine-decayed learning rate.
+ * loss_curve (may be NULL) receives each step's batch MSE in normalised
+ * units. */
+lpk_status lpk_mlp_fit(lpk_mlp *mlp, const int32_t *tx, const lpk_kepler_orbit *orbits, int32_t n_tx,
+                       const double *rx_ecef, int32_t n_rx, double epoch, double t0, double t1, int64_t n_train,
+                       int32_t steps, int32_t batch, float lr, uint64_t seed, float *loss_curve);
+/* The network's 16 raw input features of transmitter tx (one of its
+ * orbits) seen from rx_ecef at the reception times (n x 16, host memory). */
+lpk_status lpk_mlp_features(const lpk_mlp *mlp, int32_t tx, const double *rx_ecef, double epoch,
+                            const double *t_rel_utc, int64_t n, float *features);
+/* Self-check of the inference kernel's bounded tensor-core completion wait
+ * (no reference counterpart): runs the kernel on n rows with its MMAs
+ * withheld, so every completion wait gives up after `spin` polls with
+ * nothing in flight. Returns LPK_ETIMEDOUT when the give-up path reported
+ * it (the expected outcome; the context stays usable), LPK_EINVAL if a wait
+ * did not give up. */
+lpk_status lpk_mlp_wait_selftest(lpk_mlp *mlp, int64_t n, int32_t spin);
 
 /* ------------------------------------------------------------------ */
 /* Host-level mirror of src/pipeline.rs (scene -> per-band streams)     */

@@ -97,6 +97,8 @@ lpk_status build_dev_band(lpk_ctx *ctx, const lpk_band_desc *d, int64_t i0, int6
          !finite(d->clock_allan_1s)))
         return fail(ctx, LPK_EINVAL, "device clock walk needs a positive master rate and allan >= 0");
     if (d->n_post < 0 || d->n_post > 3) return fail(ctx, LPK_EINVAL, "n_post must be 0..3");
+    if (d->solver != LPK_SOLVER_REFERENCE && d->solver != LPK_SOLVER_SPLIT && d->solver != LPK_SOLVER_FP64_TUNED)
+        return fail(ctx, LPK_EINVAL, "unknown solver");
     b.epoch = d->epoch_unix;
     b.fs = d->fs_hz;
     b.lo = d->lo_hz;
@@ -627,6 +629,8 @@ lpk_status lpk_band_chunk_device(lpk_ctx *c, const lpk_band_desc *band, const in
         e = launch_split_fanout(c->split_variant, b, c->d_tx, d_active, n_active, (char *)c->d_scratch + off_recs,
                                 (float2 *)d_out, nullptr, nullptr, nullptr, c->stream);
     }
+    else if (band->solver == LPK_SOLVER_FP64_TUNED)
+        e = launch_band_fp64(b, c->d_tx, d_active, n_active, (float2 *)d_out, d_uw, c->stream);
     else
         e = launch_band_reference(b, c->d_tx, d_active, n_active, (float2 *)d_out, d_uw, c->stream);
     prof_end(c);
@@ -751,6 +755,8 @@ lpk_status lpk_band_chunk(lpk_ctx *c, const lpk_band_desc *band, const int32_t *
         e = launch_split_fanout(c->split_variant, b, c->d_tx, d_active, n_active, base + off_recs, d_out, nullptr,
                                 nullptr, nullptr, c->stream);
     }
+    else if (band->solver == LPK_SOLVER_FP64_TUNED)
+        e = launch_band_fp64(b, c->d_tx, d_active, n_active, d_out, d_uw, c->stream);
     else
         e = launch_band_reference(b, c->d_tx, d_active, n_active, d_out, d_uw, c->stream);
     prof_end(c);

@@ -72,6 +72,66 @@ __device__ __forceinline__ bool contribution(const DevTx &tx, const DevBand &b, 
     return true;
 }
 
+// x reduced modulo 2π into [-π, π] in FP64 (Cody–Waite: 2π to 24 bits, so
+// k·hi is exact for |k| < 2^29, then the double nearest 2π − hi): about
+// 3e-15 rad of error at |x| ~ 1e9 rad.
+__device__ __forceinline__ double reduce_2pi(double x) {
+    const double k = rint(x * 0.15915494309189535);
+    const double r = fma(-k, 6.2831854820251465, x);
+    return fma(-k, -1.748455600074497e-07, r);
+}
+
+// One transmitter's contribution at one sample with the all-FP64 arithmetic
+// of contribution() and the shortcuts a tuned FP64 kernel takes (within
+// tolerance of the reference, not bit-exact): both iterates' table lerps
+// scaled by 1/dt instead of divided (position_ecef_batch's form,
+// src/geometry/precomputed.rs:136-153); the carrier phase reduced modulo 2π
+// in FP64 before one FP64 sincos of the reduced angle (the reference's
+// sin/cos of ~1e9 rad take the slow reduction); the CW baseband phase (the
+// reference's f32 value, src/signal/cw.rs:41-52) reduced likewise and folded
+// into the carrier phase; the amplitude from an f32 division. Returns false
+// when the antenna gain is zero.
+__device__ __forceinline__ bool contribution_fp64(const DevTx &tx, const DevBand &b, double t_local, double tu,
+                                                  double delta, double ox, double oy, double oz, float &cr,
+                                                  float &ci) {
+    double t = tu - kEmissionLag, r = 0.0;
+#pragma unroll
+    for (int it = 0; it < 2; ++it) {  // NEWTON_ITERATIONS, src/channel/mod.rs:75-96
+        double sx, sy, sz;
+        traj_position_batch(tx, b.epoch + t, sx, sy, sz);
+        const double wtau = kEarthRate * (tu - t);
+        const double dx = (sx + wtau * sy) - ox, dy = (sy - wtau * sx) - oy, dz = sz - oz;
+        r = sqrt(dx * dx + dy * dy + dz * dz);
+        t = tu - r * b.inv_c;
+    }
+    float g = 1.0f;
+    if (b.has_antenna) {
+        g = antenna_gain(tx, b, b.epoch + t, ox, oy, oz);
+        if (g == 0.0f) return false;
+    }
+    float bre = 1.0f, bim = 0.0f;
+    double extra = 0.0;
+    if (tx.sig_kind == kCw) {
+        const float ph = tx.cw_anchored ? (float)f64_rem_euclid(tx.cw_omega * t + tx.cw_phase0, kTau)
+                                        : (float)(tx.cw_omega * t);
+        extra = reduce_2pi((double)ph);
+        if (tx.has_gate && !gate_is_on(tx, t)) bre = 0.0f;
+    } else {
+        const float2 bb = baseband(tx, t);
+        bre = bb.x;
+        bim = bb.y;
+    }
+    const double delay = r * b.inv_c;
+    const double phase = tx.neg_tau_src * (delay + delta) + kTau * (tx.carrier - b.lo) * t_local;
+    double sp, cp;
+    sincos(reduce_2pi(phase) + extra, &sp, &cp);
+    const float amp = __fdiv_rn((float)tx.amp_factor, (float)r) * g;
+    const float cpf = (float)cp, spf = (float)sp;
+    cr = amp * (bre * cpf - bim * spf);
+    ci = amp * (bre * spf + bim * cpf);
+    return true;
+}
+
 // Horizon gate (src/channel/horizon.rs:140-215, certainly_below_cutoff):
 // true only if the per-sample path would give every sample of a stretch a
 // zero antenna gain for this transmitter — its arrival elevation below the

@@ -86,6 +86,9 @@ lpk_status check_active(lpk_ctx *ctx, const int32_t *active, int32_t n_active);
 // launchers (lpk_kernels.cu)
 cudaError_t launch_band_reference(const DevBand &b, const DevTx *d_tx, const int32_t *d_active,
                                   int32_t n_active, float2 *d_out, uint32_t *d_unocc, cudaStream_t s);
+// The tuned all-FP64 fan-out (LPK_SOLVER_FP64_TUNED).
+cudaError_t launch_band_fp64(const DevBand &b, const DevTx *d_tx, const int32_t *d_active, int32_t n_active,
+                             float2 *d_out, uint32_t *d_unocc, cudaStream_t s);
 cudaError_t launch_tx_contribution(const DevBand &b, const DevTx *d_tx, int32_t tx, float2 *d_out,
                                    double *d_phase, double *d_temit, double *d_range, cudaStream_t s);
 cudaError_t launch_rx_chain(const DevBand &b, float2 *d_iq, cudaStream_t s);

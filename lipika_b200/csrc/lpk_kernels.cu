@@ -86,6 +86,49 @@ k_band_reference(const DevBand b, const DevTx *__restrict__ txs, const int32_t *
     out[j] = band_epilogue(b, acc_re, acc_im, g);
 }
 
+// The tuned all-FP64 fan-out (contribution_fp64): one thread per band
+// sample, the band's transmitters from shared memory in active-list order,
+// the sample time as the IEEE quotient without a division sequence, the
+// epilogue of k_band_reference. Within tolerance of k_band_reference.
+__global__ void __launch_bounds__(kBlock)
+k_band_fp64(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__restrict__ active, int32_t n_active,
+            float2 *__restrict__ out, uint32_t *__restrict__ unocc) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    DevTx *stx = reinterpret_cast<DevTx *>(smem_raw);
+    {
+        const int words = (int)(sizeof(DevTx) / 8);
+        for (int k = 0; k < n_active; ++k) {
+            const uint64_t *src = reinterpret_cast<const uint64_t *>(txs + active[k]);
+            uint64_t *dst = reinterpret_cast<uint64_t *>(stx + k);
+            for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = src[w];
+        }
+    }
+    __syncthreads();
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = j < b.n;
+    const int64_t g = b.i0 + (live ? j : 0);
+    const double t_local = sample_time((double)g, b.fs, __drcp_rn(b.fs));
+    const double delta = band_delta(b, live ? j : 0, t_local);
+    const double tu = t_local - delta;
+    double ox, oy, oz;
+    band_rx(b, live ? j : 0, ox, oy, oz);
+    float acc_re = 0.0f, acc_im = 0.0f;
+    for (int k = 0; k < n_active; ++k) {
+        float cr = 0.0f, ci = 0.0f;
+        const bool on = live && contribution_fp64(stx[k], b, t_local, tu, delta, ox, oy, oz, cr, ci);
+        if (on) {
+            acc_re = __fadd_rn(acc_re, cr);
+            acc_im = __fadd_rn(acc_im, ci);
+        }
+        if (b.has_antenna && unocc) {
+            unsigned any = __ballot_sync(0xffffffffu, on);
+            if ((threadIdx.x & 31) == 0 && any) atomicOr(unocc + k, 1u);
+        }
+    }
+    if (!live) return;
+    out[j] = band_epilogue(b, acc_re, acc_im, g);
+}
+
 __global__ void __launch_bounds__(kBlock)
 k_tx_contribution(const DevBand b, const DevTx *__restrict__ txs, int32_t tx_idx, float2 *__restrict__ out,
                   double *phase, double *temit, double *range) {
@@ -261,6 +304,18 @@ cudaError_t launch_band_reference(const DevBand &b, const DevTx *d_tx, const int
         if (e != cudaSuccess) return e;
     }
     k_band_reference<<<grid_for(b.n), kBlock, smem, s>>>(b, d_tx, d_active, n_active, d_out, d_unocc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_band_fp64(const DevBand &b, const DevTx *d_tx, const int32_t *d_active, int32_t n_active,
+                             float2 *d_out, uint32_t *d_unocc, cudaStream_t s) {
+    if (b.n <= 0) return cudaSuccess;
+    size_t smem = sizeof(DevTx) * (size_t)n_active;
+    if (smem > 40 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_band_fp64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    k_band_fp64<<<grid_for(b.n), kBlock, smem, s>>>(b, d_tx, d_active, n_active, d_out, d_unocc);
     return cudaGetLastError();
 }
 

@@ -75,11 +75,13 @@ struct __align__(16) AnchorRec {
     float amp0, amp1;                 // amplitude = amp0 + amp1 Δ
     int32_t flags;
     int32_t nav_pm;                   // nav sign of the tile (1 with nav off; unused with kRecNavVary)
-    int64_t sym_raw0, sym_pos0;       // framed kinds: raw symbol count at the tile start and its frame slot
-    double chip_base;                 // C/A: 1.5 x 2^52 - f0, f0 a whole chip count at or below the
-                                      // tile's first chip (floor(cp) + chip_base holds floor(cp) - f0
-                                      // in its low 32 bits, exactly)
-    int32_t chip_m0;                  // C/A: f0 mod 1023
+    int64_t sym_lo, sym_hi;           // framed kinds, one-shot frame: the symbols f0 + m of the frame
+                                      // are those with m in [sym_lo, sym_hi)
+    double chip_base;                 // C/A and framed kinds: 1.5 x 2^52 - f0, f0 a whole chip / symbol
+                                      // count at or below the tile's first one (floor(x) + chip_base
+                                      // holds floor(x) - f0 in its low 32 bits, exactly)
+    int32_t chip_m0;                  // C/A: f0 mod 1023; framed kinds: the frame slot of count f0
+                                      // (repeating frame) or f0 itself (one-shot frame)
     int32_t n_nodes;                  // most grid nodes either iterate crosses in the tile
 };
 static_assert(sizeof(AnchorRec) % 16 == 0, "AnchorRec arrays must keep 16-byte alignment");
@@ -210,7 +212,7 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
     if (exact_only) {
         r.amp0 = r.amp1 = 0.0f;
         r.guard = r.ulp_q = r.tie = 0.0;
-        r.sym_raw0 = r.sym_pos0 = 0;
+        r.sym_lo = r.sym_hi = 0;
         r.flags = kRecExact;
         return;
     }
@@ -308,19 +310,33 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
     r.ulp_q = ldexp(1.0, ilogb(fmax(fmax(fabs(b.epoch + tus), fabs(b.epoch + tue)), 1e-300)) - 52);
     const double tie = ldexp(8.0, ilogb(fmax(fmax(fabs(tus), fabs(tue)), 1.0)) - 52);
     r.tie = (8.0 * tie > r.ulp_q) ? -1.0 : tie;
-    r.sym_raw0 = 0;
-    r.sym_pos0 = 0;
+    r.sym_lo = 0;
+    r.sym_hi = 0;
     if (!exact && (tx.sig_kind == kBpsk || tx.sig_kind == kOok || tx.sig_kind == kQam16)) {
+        // tile-relative symbol index m = floor(x) - f0 as for the C/A chips;
+        // the frame slot then takes 32-bit arithmetic (frame_index,
+        // src/signal/mod.rs:109-115)
+        const double xs = (te_s - tx.epoch_rel) * tx.rate, xe = (te_e - tx.epoch_rel) * tx.rate;
+        const double f0 = floor(xs) - 2.0;
         if (tx.n_sym <= 0) {
             r.flags |= kRecGateOff;  // an empty frame is silent everywhere
+        } else if (!(fabs(f0) < 1.0e15) || !(xe - f0 + 2.0 < 1073741824.0) || tx.n_sym >= ((int64_t)1 << 30)) {
+            exact = true;
+        } else if (!tx.has_repeat && (xe + 2.0 < 0.0 || f0 >= (double)tx.n_sym)) {
+            r.flags |= kRecGateOff;  // the tile lies wholly outside the one-shot frame
         } else {
-            r.sym_raw0 = floor_to_i64((te_s - tx.epoch_rel) * tx.rate);
-            r.sym_pos0 = tx.has_repeat
-                             ? i64_rem_euclid((int64_t)((uint64_t)r.sym_raw0 + (uint64_t)tx.repeat_from), tx.n_sym)
-                             : r.sym_raw0;
-            // the per-sample slot wraps at most once: the tile must span
-            // fewer symbols than the frame holds
-            if (tx.has_repeat && !((te_e - te_s) * tx.rate + 3.0 < (double)tx.n_sym)) exact = true;
+            r.chip_base = 0x1.8p52 - f0;  // exact: |f0| < 1e15 < 2^50
+            const int64_t f0i = (int64_t)f0;
+            if (tx.has_repeat) {
+                r.chip_m0 = (int32_t)i64_rem_euclid((int64_t)((uint64_t)f0i + (uint64_t)tx.repeat_from), tx.n_sym);
+                // the per-sample slot wraps at most once: the tile must span
+                // fewer symbols than the frame holds
+                if (!(xe - f0 + 2.0 < (double)tx.n_sym)) exact = true;
+            } else {  // f0 within [-2^30, n_sym) here, so every count below fits 32 bits
+                r.chip_m0 = (int32_t)f0i;
+                r.sym_lo = -f0i;
+                r.sym_hi = tx.n_sym - f0i;
+            }
         }
     }
     if (!exact && tx.sig_kind == kCa) {  // tile-relative chip index: chip_m0 + (floor(cp) - f0)
@@ -373,12 +389,28 @@ __device__ __forceinline__ int64_t tile_sample(int64_t first, int s) {
     return first + (int64_t)(s >> 1) * (2 * THREADS) + 2 * (int64_t)threadIdx.x + (s & 1);
 }
 
-// Per-sample values shared by every transmitter of the band: local
-// reception time, clock offset, and the rounding offset of the first
-// trajectory query epoch + (tu - 70 ms), the same for every transmitter.
+// Per-sample values shared by every transmitter of the band: the UTC
+// reception time tu = t_local - Δt, its offset d from the tile's fit origin,
+// the rounding offset q0 of the first trajectory query epoch + (tu - 70 ms),
+// and psi = -2π f_lo Δt reduced modulo 2π. The carrier phase
+// -2π f (delay + Δt) + 2π (f - f_lo) t_local equals
+// -2π f delay + 2π (f - f_lo) tu - 2π f_lo Δt (t_local = tu + Δt), so the
+// part that depends on Δt alone is formed once per sample.
 struct SampleCtx {
-    double tl, dl, q0;
+    double tu, d, q0, psi;
 };
+
+// t_local and Δt of sample s of this thread (src/pipeline.rs:918-927): the
+// values the sample context was built from, recomputed where the exact
+// path needs them. Samples outside the chunk take the nearest chunk sample.
+template <int THREADS>
+__device__ __forceinline__ void sample_clock(const DevBand &b, int64_t first, int s, double rfs, double &tl,
+                                             double &dl) {
+    const int64_t j = tile_sample<THREADS>(first, s);
+    const int64_t jc = j < 0 ? 0 : (j >= b.n ? b.n - 1 : j);
+    tl = sample_time((double)(b.i0 + jc), b.fs, rfs);
+    dl = band_delta(b, jc, tl);
+}
 
 // Per-(tile, transmitter) code paths of the fast pass, chosen outside the
 // per-sample loop so that the loop body has no branches.
@@ -430,14 +462,21 @@ __device__ __forceinline__ void split_baseband(const DevTx &tx, const AnchorRec 
     } else if constexpr (K == kPassBpsk || K == kPassOok || K == kPassQam) {  // frame_index, signal/mod.rs:109-115
         const double f = __dmul_rn(__dsub_rn(te, tx.epoch_rel), tx.rate);
         const double fl = floor(f), fr = f - fl, g = guard * tx.rate;
-        ok &= fr >= g && fr <= 1.0 - g && fabs(fl) <= 9.0e15;
-        const int64_t raw = (int64_t)fl, n = tx.n_sym;
-        int64_t p = R.sym_pos0 + (raw - R.sym_raw0);  // repeating frame: at most one wrap per tile
-        p -= p >= n ? n : 0;
-        p += p < 0 ? n : 0;
-        const bool on = tx.has_repeat ? true : (raw >= 0 && raw < n);
-        p = tx.has_repeat ? p : raw;
-        p = p < 0 ? 0 : (p >= n ? n - 1 : p);  // keeps the load in bounds; `on` masks the value
+        ok &= fr >= g && fr <= 1.0 - g;
+        // m = floor(f) - f0, read from the low word of an exact add (the
+        // tile's fit range keeps it small); samples outside the fit range
+        // are redone exactly, so only their load has to stay in bounds
+        const uint32_t m = (uint32_t)__double2loint(__dadd_rn(fl, R.chip_base));
+        const uint32_t n = (uint32_t)tx.n_sym;
+        uint32_t p = (uint32_t)R.chip_m0 + m;
+        bool on;
+        if (tx.has_repeat) {  // uniform over the block
+            p -= p >= n ? n : 0u;  // at most one wrap per tile
+            on = true;
+        } else {
+            on = (int32_t)m >= (int32_t)R.sym_lo && (int32_t)m < (int32_t)R.sym_hi;
+        }
+        p = p < n ? p : 0u;  // keeps the load in bounds; `on` masks the value
         if constexpr (K == kPassBpsk) {
             bre = on ? (float)__ldg(tx.pm + p) : 0.0f;
         } else if constexpr (K == kPassOok) {
@@ -472,7 +511,7 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
                                            unsigned fit, float *ar, float *ai, unsigned &redo, int64_t first,
                                            double *dbg_phase, double *dbg_temit, double *dbg_delay,
                                            const DevBand *acc_band = nullptr, double *acc = nullptr) {
-    const double tu0 = R.tu0, k0 = R.k0;
+    const double k0 = R.k0;
     // A rounding error never exceeds half an ulp, so "|(|err| - half)| > tie"
     // (not within `tie` of a tie) is |err| < half - tie; half and tie are
     // powers of two, so the difference is exact (tie < 0: always true).
@@ -486,8 +525,7 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         const SampleCtx &c = sc[s];
-        const double tu = __dsub_rn(c.tl, c.dl);  // src/pipeline.rs:927
-        const double d = tu - tu0;
+        const double tu = c.tu, d = c.d;
         double t1s, poly1, k1;
         if constexpr (NK > 0) {
             const double q = __dadd_rn(epoch, __dsub_rn(tu, kEmissionLag));
@@ -525,30 +563,66 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
         const double delay = fma(k1, e1 - t1s, poly1);
         const double te = tu - delay;
         float bre, bim;
-        split_baseband<K>(tx, R, te, guard, ok, bre, bim);
+        double rb = 0.0;
+        if constexpr (K == kPassCw) {
+            // CW (cw.rs:41-52): the reference rounds its baseband phase ω·t to
+            // f32 (up to ~1e6 rad over a minute) and takes an f32 sin/cos of
+            // that value; here the f32 value is reduced exactly in FP64
+            // (Cody–Waite, as below) and folded into the carrier phase, so
+            // one sin/cos of the sum replaces the f32 sincos of a large
+            // argument and the complex product
+            const double pb = (double)(tx.cw_anchored
+                                           ? (float)f64_rem_euclid(__dadd_rn(__dmul_rn(tx.cw_omega, te), tx.cw_phase0),
+                                                                   kTau)
+                                           : (float)__dmul_rn(tx.cw_omega, te));
+            const double kb = rint(pb * 0.15915494309189535);
+            rb = fma(-kb, 6.2831854820251465, pb);
+            rb = fma(-kb, -1.748455600074497e-07, rb);
+            bre = 1.0f;
+            bim = 0.0f;
+        } else {
+            split_baseband<K>(tx, R, te, guard, ok, bre, bim);
+        }
         // carrier phase −2π f (delay + Δt) + 2π (f − f_lo) t_local, reduced mod 2π
         // (Cody–Waite: 2π to 24 bits, kq·hi exact, then 2π − hi); the f32
         // rounding of the reduced phase is < 1.2e-7 rad, below __sincosf's own error
-        const double phase = fma(tau_if, c.tl, nts * (delay + c.dl));
+        const double phase = fma(nts, delay, fma(tau_if, tu, c.psi));
         const double kq = rint(phase * 0.15915494309189535);
         double rr = fma(-kq, 6.2831854820251465, phase);
         rr = fma(-kq, -1.748455600074497e-07, rr);
+        double rt = rr;  // the angle of the sin/cos: the carrier phase, plus the baseband phase for CW
+        if constexpr (K == kPassCw) {  // both parts in [-π, π]: one wrap brings the sum back
+            rt += rb;
+            rt += rt > 3.141592653589793 ? -6.283185307179586 : (rt < -3.141592653589793 ? 6.283185307179586 : 0.0);
+        }
         float sn, cs;
-        __sincosf((float)rr, &sn, &cs);
+        __sincosf((float)rt, &sn, &cs);
         // f32 arithmetic spelled out (no contraction choices left to the
         // compiler), so every kernel that inlines this pass agrees bit for bit
         const float amp = __fmaf_rn(amp1, __double2float_rn(d), amp0);
-        const float vre = __fmaf_rn(bre, cs, __fmul_rn(-bim, sn)), vim = __fmaf_rn(bre, sn, __fmul_rn(bim, cs));
+        float vre, vim;
+        if constexpr (K == kPassCw) {
+            vre = cs;
+            vim = sn;
+        } else if constexpr (K == kPassQam) {
+            vre = __fmaf_rn(bre, cs, __fmul_rn(-bim, sn));
+            vim = __fmaf_rn(bre, sn, __fmul_rn(bim, cs));
+        } else {  // real baseband (±1 or 0/1)
+            vre = __fmul_rn(bre, cs);
+            vim = __fmul_rn(bre, sn);
+        }
         ok &= (fit >> s) & 1u;
         if constexpr (ACC) {
             if (ok) {
                 const DevBand &b = *acc_band;
+                double tl, dl;
+                sample_clock<THREADS>(b, first, s, __drcp_rn(b.fs), tl, dl);
                 double te_ref, r_ref;
                 solve_reference(tx, tu, b.rx[0], b.rx[1], b.rx[2], epoch, 2, b.inv_c, te_ref, r_ref);
                 const double delay_ref = __dmul_rn(r_ref, b.inv_c);
                 const double tif = __dmul_rn(kTau, __dsub_rn(tx.carrier, b.lo));
-                const double ph_ref = __dadd_rn(__dmul_rn(tx.neg_tau_src, __dadd_rn(delay_ref, c.dl)),
-                                                __dmul_rn(tif, c.tl));
+                const double ph_ref = __dadd_rn(__dmul_rn(tx.neg_tau_src, __dadd_rn(delay_ref, dl)),
+                                                __dmul_rn(tif, tl));
                 double dp = rr - remainder(ph_ref, kTau);
                 dp -= kTau * rint(dp * 0.15915494309189535);
                 acc[0] = fmax(acc[0], fabs(delay - delay_ref));
@@ -594,6 +668,7 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
     unsigned live = 0, fit = 0;
     const double tu0 = n_active > 0 ? srec[0].tu0 : 0.0, tu_hi = n_active > 0 ? srec[0].tu_hi : 0.0;
     const double rfs = __drcp_rn(b.fs);
+    const double nlo = -kTau * b.lo;  // -2π f_lo
     static_assert(S % 2 == 0, "samples are held in adjacent pairs");
 #pragma unroll
     for (int s = 0; s < S; ++s) {
@@ -609,7 +684,7 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
         const double tu = __dsub_rn(tl, dl);                      // :927
         const double t0q = __dsub_rn(tu, kEmissionLag);
         const double s0 = __dadd_rn(b.epoch, t0q);
-        sc[s] = SampleCtx{tl, dl, __dsub_rn(__dsub_rn(s0, b.epoch), t0q)};
+        sc[s] = SampleCtx{tu, tu - tu0, __dsub_rn(__dsub_rn(s0, b.epoch), t0q), reduce_2pi(nlo * dl)};
         live |= (unsigned)lv << s;
         // the fit range depends only on the tile: the same for every
         // transmitter (the pass sees `fit & live`: a sample outside the
@@ -628,7 +703,7 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
 #pragma unroll
         for (int s = 0; s < S; ++s) {
             if (!((live >> s) & 1u)) continue;
-            const double tu = __dsub_rn(sc[s].tl, sc[s].dl);
+            const double tu = sc[s].tu;
             fin = fin && isfinite(tu);
             lo = fmin(lo, tu);
             hi = fmax(hi, tu);
@@ -694,9 +769,9 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
         for (int s = 0; s < S; ++s) {  // the exact path: rare samples, or whole exact tiles
             if (!((redo >> s) & 1u)) continue;
             float cr = 0.0f, ci = 0.0f;
-            double ph = 0.0, te = 0.0, rg = 0.0;
-            const bool on = contribution(T, b, sc[s].tl, __dsub_rn(sc[s].tl, sc[s].dl), sc[s].dl, b.rx[0], b.rx[1],
-                                         b.rx[2], cr, ci, &ph, &te, &rg);
+            double ph = 0.0, te = 0.0, rg = 0.0, tl, dl;
+            sample_clock<THREADS>(b, first, s, rfs, tl, dl);
+            const bool on = contribution(T, b, tl, sc[s].tu, dl, b.rx[0], b.rx[1], b.rx[2], cr, ci, &ph, &te, &rg);
             if constexpr (UNOCC) {
                 if (on && !gate_off) atomicOr(b.unocc_words + k, 1u);
             } else {

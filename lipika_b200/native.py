@@ -7,6 +7,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 
 import numpy as np
 
@@ -27,11 +28,11 @@ LPK_TX_TRAJ_STATIONARY, LPK_TX_TRAJ_PRECOMPUTED = 0, 1
 LPK_CLOCK_HOST, LPK_CLOCK_DETERMINISTIC, LPK_CLOCK_DEVICE_WALK = 0, 1, 2
 LPK_RX_STATIONARY, LPK_RX_PER_SAMPLE = 0, 1
 LPK_POST_GAIN, LPK_POST_NONLINEARITY, LPK_POST_ADC = 0, 1, 2
-LPK_SOLVER_REFERENCE, LPK_SOLVER_SPLIT = 0, 1
+LPK_SOLVER_REFERENCE, LPK_SOLVER_SPLIT, LPK_SOLVER_FP64_TUNED = 0, 1, 2
 LPK_NOISE_OFF, LPK_NOISE_ON, LPK_GEN_DEVICE_CLOCK, LPK_GEN_SPLIT, LPK_GEN_AUTOTUNE = 0, 1, 2, 4, 8
 LPK_START_LAG, LPK_START_GEOMETRIC, LPK_START_LEARNED = 0, 1, 2
 LPK_ITER_FIXED_POINT, LPK_ITER_NEWTON = 0, 1
-MLP_N_FEATURES, MLP_N_PARAMS, MLP_N_NORM = 8, 4801, 18
+MLP_N_FEATURES, MLP_N_PARAMS, MLP_N_NORM = 16, 9473, 34
 
 
 class LpkError(RuntimeError):
@@ -174,15 +175,19 @@ SIGNATURES = {
     "lpk_generate_scene": (C.c_int32, [_VP, C.c_uint64, C.c_double, C.c_int32, UNIT_SINK_FN, _VP]),
     "lpk_solve_converged": (C.c_int32, [_VP, C.c_int32, _D, C.c_double, _D, C.c_int64, C.c_double, C.c_int32,
                                         C.c_int32, C.c_int32, _VP, _D, _I32, _F]),
-    "lpk_solve_features": (C.c_int32, [_VP, C.c_int32, _D, C.c_double, _D, C.c_int64, _F]),
+    "lpk_solve_converged_scene": (C.c_int32, [_VP, _I32, _I32, _D, C.c_int32, C.c_double, _D, C.c_int64,
+                                              C.c_double, C.c_int32, C.c_int32, C.c_int32, _VP, _D, _I32, _F, _D]),
+    "lpk_mlp_features": (C.c_int32, [_VP, C.c_int32, _D, C.c_double, _D, C.c_int64, _F]),
+    "lpk_mlp_set_orbits": (C.c_int32, [_VP, _I32, C.POINTER(KeplerOrbit), C.c_int32]),
+    "lpk_mlp_wait_selftest": (C.c_int32, [_VP, C.c_int64, C.c_int32]),
     "lpk_mlp_create": (C.c_int32, [_VP, C.c_uint64, C.POINTER(_VP)]),
     "lpk_mlp_destroy": (None, [_VP]),
     "lpk_mlp_get_params": (C.c_int32, [_VP, _F, _F]),
     "lpk_mlp_set_params": (C.c_int32, [_VP, _F, _F]),
     "lpk_mlp_forward": (C.c_int32, [_VP, _F, C.c_int64, _F]),
     "lpk_mlp_loss_grad": (C.c_int32, [_VP, _F, _F, C.c_int64, _D, _F]),
-    "lpk_mlp_fit": (C.c_int32, [_VP, C.c_int32, _D, C.c_double, C.c_double, C.c_double, C.c_int64, C.c_int32,
-                                C.c_int32, C.c_float, C.c_uint64, _F]),
+    "lpk_mlp_fit": (C.c_int32, [_VP, _I32, C.POINTER(KeplerOrbit), C.c_int32, _D, C.c_int32, C.c_double,
+                                C.c_double, C.c_double, C.c_int64, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _F]),
     "lpk_clock_new": (C.c_int32, [C.POINTER(A.ClockCfg), C.c_double, C.c_double, C.c_uint64, C.POINTER(_VP)]),
     "lpk_clock_delta_t": (C.c_int32, [_VP, _D, C.c_int64, _D]),
     "lpk_clock_free": (None, [_VP]),
@@ -222,15 +227,25 @@ def dptr(a):
 
 
 class Context:
-    """An lpk_ctx: one CUDA device, its stream and its uploaded scene."""
+    """An lpk_ctx: one CUDA device, its stream and its uploaded scene.
+
+    Objects made on a context (a scene, a batch, a network) register here
+    and are closed before the context itself: their C handles refer to it."""
 
     def __init__(self, device: int = 0):
         h = _VP()
         check(lib().lpk_ctx_create(C.byref(h), device))
         self.h = h
         self.device = device
+        self._deps = weakref.WeakSet()
+
+    def adopt(self, obj):
+        """Close obj (it has a close()) before this context closes."""
+        self._deps.add(obj)
 
     def close(self):
+        for d in list(getattr(self, "_deps", ())):
+            d.close()
         if getattr(self, "h", None):
             try:
                 lib().lpk_ctx_destroy(self.h)
@@ -281,6 +296,7 @@ class Batch:
         h = _VP()
         ctx.check(lib().lpk_batch_create(ctx.h, arr, len(units), float(round_s), C.byref(h)))
         self.h = h
+        ctx.adopt(self)
         self.n_units = len(units)
         self.n_rounds = int(lib().lpk_batch_n_rounds(h))
         self._caps = [max([self.extent(r, u)[1] for r in range(min(self.n_rounds, 2))] + [1])
@@ -361,6 +377,7 @@ class Mlp:
         h = _VP()
         ctx.check(lib().lpk_mlp_create(ctx.h, seed & 0xFFFFFFFFFFFFFFFF, C.byref(h)))
         self.h = h
+        ctx.adopt(self)
 
     def close(self):
         if getattr(self, "h", None):
@@ -398,12 +415,29 @@ class Mlp:
         self.ctx.check(lib().lpk_mlp_loss_grad(self.h, _fp(x), _fp(t), len(x), C.byref(loss), _fp(g)))
         return loss.value, g
 
-    def fit(self, tx, rx_ecef, epoch, t0, t1, n_train=1 << 18, steps=1500, batch=4096, lr=3e-3, seed=1):
-        rx = np.ascontiguousarray(rx_ecef, np.float64)
+    def fit(self, txs, orbits, rx_ecef, epoch, t0, t1, n_train=1 << 21, steps=2000, batch=4096, lr=3e-3, seed=1):
+        """Train the scene's surrogate: txs (uploaded indices) with their
+        circular orbits (KeplerOrbit each), rx_ecef (n_rx, 3) receivers,
+        reception times in [t0, t1). Returns the per-step batch loss."""
+        tx = np.ascontiguousarray(np.asarray(txs, np.int32))
+        orb = (KeplerOrbit * len(orbits))(*orbits)
+        rx = np.ascontiguousarray(np.asarray(rx_ecef, np.float64).reshape(-1, 3))
         curve = np.zeros(steps, np.float32)
-        self.ctx.check(lib().lpk_mlp_fit(self.h, tx, dptr(rx), epoch, t0, t1, n_train, steps, batch, lr,
-                                         seed & 0xFFFFFFFFFFFFFFFF, _fp(curve)))
+        self.ctx.check(lib().lpk_mlp_fit(self.h, tx.ctypes.data_as(_I32), orb, len(tx), dptr(rx), len(rx), epoch, t0,
+                                         t1, n_train, steps, batch, lr, seed & 0xFFFFFFFFFFFFFFFF, _fp(curve)))
         return curve
+
+    def set_orbits(self, txs, orbits):
+        tx = np.ascontiguousarray(np.asarray(txs, np.int32))
+        orb = (KeplerOrbit * len(orbits))(*orbits)
+        self.ctx.check(lib().lpk_mlp_set_orbits(self.h, tx.ctypes.data_as(_I32), orb, len(tx)))
+
+    def features(self, tx, rx_ecef, epoch, t_rel_utc):
+        t = np.ascontiguousarray(t_rel_utc, np.float64)
+        rx = np.ascontiguousarray(rx_ecef, np.float64)
+        f = np.zeros((len(t), MLP_N_FEATURES), np.float32)
+        self.ctx.check(lib().lpk_mlp_features(self.h, tx, dptr(rx), epoch, dptr(t), len(t), _fp(f)))
+        return f
 
 
 def solve_converged(ctx: Context, tx, rx_ecef, epoch, t_rel_utc, tol=1e-13, max_iter=12,
@@ -420,9 +454,34 @@ def solve_converged(ctx: Context, tx, rx_ecef, epoch, t_rel_utc, tol=1e-13, max_
     return te, it, err
 
 
-def solve_features(ctx: Context, tx, rx_ecef, epoch, t_rel_utc):
+def solve_converged_scene(ctx: Context, tx, rx_idx, rx_ecef, epoch, t_rel_utc, tol=1e-13, max_iter=12,
+                          scheme=LPK_ITER_NEWTON, start=LPK_START_LAG, mlp: "Mlp | None" = None):
+    """Converged emission solve over (transmitter, receiver) pairs:
+    (t_emit, iterations, |start - converged| in s, device ms)."""
     t = np.ascontiguousarray(t_rel_utc, np.float64)
-    rx = np.ascontiguousarray(rx_ecef, np.float64)
-    f = np.zeros((len(t), MLP_N_FEATURES), np.float32)
-    ctx.check(lib().lpk_solve_features(ctx.h, tx, dptr(rx), epoch, dptr(t), len(t), _fp(f)))
-    return f
+    txa = np.ascontiguousarray(np.asarray(tx, np.int32))
+    rxa = np.ascontiguousarray(np.asarray(rx_idx, np.int32))
+    rx = np.ascontiguousarray(np.asarray(rx_ecef, np.float64).reshape(-1, 3))
+    te = np.zeros(len(t))
+    it = np.zeros(len(t), np.int32)
+    err = np.zeros(len(t), np.float32)
+    ms = C.c_double()
+    ctx.check(lib().lpk_solve_converged_scene(ctx.h, txa.ctypes.data_as(_I32), rxa.ctypes.data_as(_I32), dptr(rx),
+                                              len(rx), epoch, dptr(t), len(t), tol, max_iter, scheme, start,
+                                              mlp.h if mlp is not None else None, dptr(te), it.ctypes.data_as(_I32),
+                                              _fp(err), C.byref(ms)))
+    return te, it, err, ms.value
+
+
+def scene_orbits(scene):
+    """(transmitter indices, KeplerOrbit per index) of a scene's transmitters
+    on circular Keplerian orbits: the inputs of the scene's surrogate."""
+    txs, orbits = [], []
+    for i, t in enumerate(scene.transmitters):
+        if t.trajectory.kind != "circular_keplerian":
+            continue
+        p = t.trajectory.params
+        txs.append(i)
+        orbits.append(KeplerOrbit(p["semi_major_axis_m"], p["inclination_deg"], p["raan_deg"],
+                                  p["true_anomaly_deg_at_epoch"], p.get("epoch_unix", scene.epoch_unix)))
+    return txs, orbits

@@ -110,6 +110,7 @@ class Prepared:
         h = C.c_void_p()
         N.check(N.lib().lpk_scene_prepare(self.ctx.h, C.byref(self.cs.cfg), C.byref(h)), self.ctx.h)
         self.h = h
+        self.ctx.adopt(self)
 
     def close(self):
         if getattr(self, "h", None):

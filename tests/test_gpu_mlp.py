@@ -1,7 +1,10 @@
 """The learned warm start of the converged emission solve: tensor-core
-forward and gradient kernels against the CPU restatement, the converged
-solver against the oracle's 80-bit solve, and what the trained network
-gains over starting where the reference starts (t - 70 ms)."""
+forward and training-gradient kernels against the CPU restatement, the
+network's feature layer against its float64 restatement, the bounded
+tensor-core wait's give-up path, the converged solver against the oracle's
+80-bit solve, and what the scene's trained network gains over starting
+where the reference starts (t - 70 ms) on the 64-transmitter x 16-receiver
+scene."""
 import ctypes as C
 
 import numpy as np
@@ -16,7 +19,7 @@ from tests import scenes
 pytestmark = pytest.mark.gpu
 
 GRAD_RTOL = 1e-2     # norm-wise, per parameter tensor (BF16 operands, FP32 accumulation)
-FORWARD_ATOL = 2e-3  # outputs are O(1)
+FORWARD_ATOL = 3e-3  # outputs are O(1)
 # Converged FP64 solve vs the oracle's 80-bit solve: two ulps of the
 # emission time, plus 2 fs for the oracle's own query epoch + t, which 80-bit
 # arithmetic rounds to 1.2e-10 s (a few 1e-16 s of delay). Far below 1 ps.
@@ -39,6 +42,18 @@ def dual(ctx):
     prep.close()
 
 
+@pytest.fixture(scope="module")
+def sky():
+    """The 64-transmitter x 16-receiver scene (60 s), its receivers, and a
+    context of its own (a context holds one uploaded scene)."""
+    c = N.Context(0)
+    sc = scenes.config_c4(duration_s=60.0)
+    prep = P.Prepared(sc, c)
+    rx = np.array([prep.band_desc(r, 0, 2026, r).rx_ecef[:] for r in range(len(sc.receivers))])
+    yield sc, prep, rx, c
+    c.close()
+
+
 def _params(seed):
     rng = np.random.default_rng(seed)
     p = rng.uniform(-0.3, 0.3, M.N_PARAMS).astype(np.float32)
@@ -51,7 +66,7 @@ def test_forward_matches_cpu_restatement(ctx):
     p = _params(1)
     m.set_params(p)
     rng = np.random.default_rng(2)
-    x = rng.normal(size=(1000, M.N_F)).astype(np.float32)  # not a multiple of the 16-row warp tile
+    x = rng.normal(size=(1000, M.N_F)).astype(np.float32)  # not a multiple of the 128-row tile
     y = m.forward(x)
     yr, _ = M.forward(p, x)
     assert np.max(np.abs(y - yr)) <= FORWARD_ATOL, np.max(np.abs(y - yr))
@@ -94,10 +109,50 @@ def test_gradient_matches_cpu_restatement(ctx, n):
     loss, g = m.loss_grad(x, t)
     lr, gr = M.loss_grad(p, x, t)
     assert abs(loss - lr) <= 1e-4 * abs(lr)
-    for name, a, b in (("W1", M.OFF_W1, M.OFF_B1), ("b1", M.OFF_B1, M.OFF_W2), ("W2", M.OFF_W2, M.OFF_B2),
-                       ("b2", M.OFF_B2, M.OFF_W3), ("w3", M.OFF_W3, M.OFF_B3), ("b3", M.OFF_B3, M.N_PARAMS)):
+    for name, a, b in M.TENSORS:
         err = np.linalg.norm(g[a:b] - gr[a:b]) / max(np.linalg.norm(gr[a:b]), 1e-30)
         assert err <= GRAD_RTOL, (name, n, err)
+    m.close()
+
+
+def test_wait_gives_up_and_context_stays_usable(ctx):
+    """The inference kernel with its MMAs withheld: every bounded completion
+    wait runs out (nothing is in flight), the call reports LPK_ETIMEDOUT,
+    and the next real forward on the same context is correct."""
+    import time
+    m = N.Mlp(ctx, seed=7)
+    p = _params(5)
+    m.set_params(p)
+    t0 = time.perf_counter()
+    code = N.lib().lpk_mlp_wait_selftest(m.h, 5000, 1 << 12)
+    assert code == N.LPK_ETIMEDOUT
+    assert b"gave up" in N.lib().lpk_last_error(ctx.h)
+    assert time.perf_counter() - t0 < 5.0
+    x = np.random.default_rng(6).normal(size=(777, M.N_F)).astype(np.float32)
+    yr, _ = M.forward(p, x)
+    assert np.max(np.abs(m.forward(x) - yr)) <= FORWARD_ATOL
+    m.close()
+
+
+def test_features_match_cpu_restatement(sky):
+    """The analytic feature layer (orbit state from the elements, line of
+    sight, range, range rate) against its float64 restatement."""
+    sc, prep, rx, ctx = sky
+    txs, orbits = N.scene_orbits(sc)
+    m = N.Mlp(ctx, seed=1)
+    m.set_orbits(txs, orbits)
+    t = np.linspace(0.0, 60.0, 4001)
+    for k in (0, 17, 40, 63):
+        o = orbits[k]
+        f = m.features(txs[k], rx[k % len(rx)], sc.epoch_unix, t)
+        fr, _ = M.features((o.semi_major_axis_m, o.inclination_deg, o.raan_deg, o.true_anomaly_deg_at_epoch),
+                           o.epoch_unix, rx[k % len(rx)], sc.epoch_unix, t)
+        scale = np.maximum(np.abs(fr), 1e-30)
+        rel = np.abs(f - fr) / scale
+        # FP32 features: relative error at float rounding, except where a
+        # component crosses zero (then absolute, against the column's size)
+        col = np.max(np.abs(fr), axis=0)
+        assert np.all((rel <= 2e-6) | (np.abs(f - fr) <= 2e-6 * col)), k
     m.close()
 
 
@@ -119,32 +174,59 @@ def test_converged_solve_matches_oracle_truth(ctx, dual, scheme):
         assert np.max(excess) <= 0.0, (tx, np.max(np.abs(te - ote)))
 
 
-def test_learned_start_cuts_iterations(ctx, dual):
+def test_scene_solve_equals_pairwise_solve(ctx, dual):
+    """lpk_solve_converged_scene (per-sample transmitter and receiver) gives
+    the bits of lpk_solve_converged (one pair per call)."""
     sc, prep, rx, epoch = dual
+    rng = np.random.default_rng(3)
+    n = 5000
+    tx = rng.integers(0, len(sc.transmitters), n).astype(np.int32)
+    rx2 = np.stack([rx, rx + np.array([1000.0, -2000.0, 500.0])])
+    ri = rng.integers(0, 2, n).astype(np.int32)
+    t = rng.uniform(0.0, 119.0, n)
+    te, it, _, ms = N.solve_converged_scene(ctx, tx, ri, rx2, epoch, t, tol=1e-14, scheme=N.LPK_ITER_NEWTON,
+                                            start=N.LPK_START_GEOMETRIC)
+    assert ms > 0.0
+    for k in range(len(sc.transmitters)):
+        for r in range(2):
+            sel = (tx == k) & (ri == r)
+            te1, it1, _ = N.solve_converged(ctx, k, rx2[r], epoch, t[sel], tol=1e-14, scheme=N.LPK_ITER_NEWTON,
+                                            start=N.LPK_START_GEOMETRIC)
+            assert np.array_equal(te[sel], te1) and np.array_equal(it[sel], it1)
+
+
+def test_learned_start_cuts_iterations(sky):
+    """One network for the 64 transmitters x 16 receivers, trained on 2^21
+    converged solves, against the reference's start (t - 70 ms) and the
+    table's geometric range, on fresh (transmitter, receiver, time) triples:
+    fewer map evaluations than the lag start under both schemes, no more
+    than the geometric start, every start converging to the same times."""
+    sc, prep, rx, ctx = sky
+    txs, orbits = N.scene_orbits(sc)
+    m = N.Mlp(ctx, seed=5)
+    curve = m.fit(txs, orbits, rx, sc.epoch_unix, 0.0, 60.0, n_train=1 << 21, steps=2000, batch=4096, lr=3e-3,
+                  seed=9)
+    assert curve[-50:].mean() < 0.01 * curve[:20].mean(), (curve[:5], curve[-5:])
     rng = np.random.default_rng(11)
-    t = np.sort(rng.uniform(0.0, 120.0, 20000))
+    n = 200_000
+    tx = np.asarray(txs, np.int32)[rng.integers(0, len(txs), n)]
+    ri = rng.integers(0, len(rx), n).astype(np.int32)
+    t = rng.uniform(0.0, 60.0, n)
     report = {}
-    for tx, label in ((0, "LEO 437 MHz"), (1, "GPS PRN 1")):
-        m = N.Mlp(ctx, seed=5)
-        curve = m.fit(tx, rx, epoch, 0.0, 120.0, n_train=1 << 18, steps=1500, batch=4096, lr=3e-3, seed=9)
-        assert curve[-50:].mean() < 0.02 * curve[:20].mean(), (curve[:5], curve[-5:])
-        out = {}
-        for scheme, sname in ((N.LPK_ITER_FIXED_POINT, "fixed-point"), (N.LPK_ITER_NEWTON, "newton")):
-            res = {}
-            for start, lname in ((N.LPK_START_LAG, "lag"), (N.LPK_START_GEOMETRIC, "geometric"),
-                                 (N.LPK_START_LEARNED, "learned")):
-                te, it, err = N.solve_converged(ctx, tx, rx, epoch, t, tol=1e-13, max_iter=12, scheme=scheme,
-                                                start=start, mlp=m)
-                assert np.all(it > 0)
-                res[lname] = (te, float(it.mean()), float(np.median(err)), float(np.max(err)))
-            # every start converges to the same emission times
-            for lname in ("geometric", "learned"):
-                assert np.max(np.abs(res[lname][0] - res["lag"][0])) <= 2e-13
-            out[sname] = {k: {"mean_evals": v[1], "median_start_err_s": v[2], "max_start_err_s": v[3]}
-                          for k, v in res.items()}
-            assert res["learned"][1] < res["lag"][1]
-            assert res["learned"][2] < 0.1 * res["geometric"][2]
-        assert out["fixed-point"]["learned"]["mean_evals"] < out["fixed-point"]["geometric"]["mean_evals"]
-        report[label] = out
-        m.close()
-    print("converged solve, tol 1e-13 s:", report)
+    for scheme, sname in ((N.LPK_ITER_FIXED_POINT, "fixed-point"), (N.LPK_ITER_NEWTON, "newton")):
+        res = {}
+        for start, lname in ((N.LPK_START_LAG, "lag"), (N.LPK_START_GEOMETRIC, "geometric"),
+                             (N.LPK_START_LEARNED, "learned")):
+            te, it, err, _ = N.solve_converged_scene(ctx, tx, ri, rx, sc.epoch_unix, t, tol=1e-12, max_iter=12,
+                                                     scheme=scheme, start=start, mlp=m)
+            assert np.all(it > 0)
+            res[lname] = (te, float(it.mean()), float(np.median(err)), float(np.max(err)))
+        for lname in ("geometric", "learned"):
+            assert np.max(np.abs(res[lname][0] - res["lag"][0])) <= 2e-12
+        report[sname] = {k: {"mean_evals": v[1], "median_start_err_s": v[2], "max_start_err_s": v[3]}
+                         for k, v in res.items()}
+        assert res["learned"][1] < res["lag"][1]
+        assert res["learned"][1] <= res["geometric"][1] + 1e-9
+        assert res["learned"][2] < 0.1 * res["geometric"][2]
+    print("converged solve, |residual| < 1e-12 s, 64 x 16 scene:", report)
+    m.close()

@@ -156,3 +156,36 @@ def test_sixty_four_transmitter_window_matches_oracle(ctx):
         assert err <= IQ_RTOL, (w, err)
     print(f"64 x 16 scene, 0.2 s: worst {worst:.2e} of max|oracle|")
     prep.close()
+
+
+@pytest.mark.parametrize("name", ["c1", "c4"])
+def test_tuned_fp64_kernel_within_tolerance(ctx, name):
+    """The tuned all-FP64 fan-out (LPK_SOLVER_FP64_TUNED: lerp by 1/dt,
+    phases reduced modulo 2π before one FP64 sincos) against the
+    reference-exact FP64 kernel on every band of the scene: IQ within
+    1e-5 x max|IQ|."""
+    import torch
+    sc = {"c1": lambda: W.config_c1(duration_s=8.0, noise=False),
+          "c4": lambda: W.config_c4(duration_s=4.0, noise=False)}[name]()
+    prep = P.Prepared(sc, ctx)
+    L = N.lib()
+    worst = 0.0
+    for w, (r, b) in enumerate(prep.work()):
+        d = prep.band_desc(r, b, 2026, w)
+        d.clock_mode = N.LPK_CLOCK_DEVICE_WALK
+        n = prep.n_samples(r, b)
+        act = (C.c_int32 * max(len(prep.active(r, b)), 1))(*prep.active(r, b))
+        outs = []
+        for solver in (N.LPK_SOLVER_REFERENCE, N.LPK_SOLVER_FP64_TUNED):
+            d.solver = solver
+            o = torch.zeros(2 * n, dtype=torch.float32, device="cuda")
+            ctx.check(L.lpk_band_chunk_device(ctx.h, C.byref(d), act, len(prep.active(r, b)), 0, n, None, None,
+                                              o.data_ptr(), None))
+            ctx.check(L.lpk_sync(ctx.h))
+            outs.append(o.view(n, 2).double())
+        scale = float(torch.linalg.vector_norm(outs[0], dim=1).max())
+        err = float(torch.linalg.vector_norm(outs[1] - outs[0], dim=1).max()) / scale
+        worst = max(worst, err)
+        assert err <= IQ_RTOL, (w, err)
+    print(f"{name}: tuned FP64 vs reference FP64, worst {worst:.2e} of max|IQ|")
+    prep.close()

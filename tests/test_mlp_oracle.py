@@ -28,7 +28,8 @@ def test_unquantised_gradient_matches_finite_differences():
     x = rng.normal(size=(37, M.N_F))
     t = rng.normal(size=37)
     _, g = M.loss_grad(p, x, t, quantize=False)
-    idx = np.r_[rng.choice(M.N_PARAMS, 60, replace=False), M.OFF_B3, M.OFF_W1, M.OFF_W2 + 5]
+    idx = np.r_[rng.choice(M.N_PARAMS, 60, replace=False), M.OFF_B4, M.OFF_W1, M.OFF_W2 + 5, M.OFF_W3 + 7,
+                M.OFF_W4 + 3]
     for i in idx:
         h = 1e-6
         pp, pm = p.copy(), p.copy()
@@ -46,3 +47,14 @@ def test_quantised_gradient_stays_close_to_exact():
     _, gq = M.loss_grad(p, x, t)
     _, g = M.loss_grad(p, x, t, quantize=False)
     assert np.linalg.norm(gq - g) <= 0.05 * np.linalg.norm(g)
+
+
+def test_orbit_state_velocity_is_the_derivative():
+    orbit = (7.0e6, 51.6, 100.0, 270.0)
+    e = np.array([0.0, 13.7, 59.9])
+    h = 1e-3
+    p0, v0 = M.orbit_state(orbit, e)
+    pp, _ = M.orbit_state(orbit, e + h)
+    pm, _ = M.orbit_state(orbit, e - h)
+    assert np.max(np.abs((pp - pm) / (2 * h) - v0)) < 1e-3  # m/s
+    assert np.allclose(np.linalg.norm(p0, axis=1), 7.0e6)
