@@ -22,6 +22,8 @@
 // (Cody–Waite), then sin/cos, amplitude and the complex MAC in FP32.
 #pragma once
 
+#include <cstddef>
+
 #include "lpk_contrib.cuh"
 
 namespace lpk {
@@ -60,31 +62,43 @@ constexpr double kSplitMargin = 1e-5;  // s
 enum : int32_t { kRecExact = 1, kRecNavVary = 2, kRecGateOff = 4, kRecCaWide = 8 };
 
 struct __align__(16) AnchorRec {
-    double tu0, tu_hi;                // fit range; Δ origin tu0
-    // An iterate's query crosses up to kSplitNodes grid nodes inside a tile
-    // (a tile up to 3 grid steps long): piece p >= 1 starts at the p-th node
-    // (absolute query time, kSplitInf when absent). Pieces 0-1 live here,
-    // pieces 2-3 of a tile with n_nodes > 1 in its AnchorExt.
-    double node0, node1;              // first node of each iterate
-    double p0[2][3], p1[2][3];        // first- / second-iterate delay pieces 0-1 (unrounded query)
-    double k0, k1[2];                 // ∂delay/∂(query time): first iterate, second iterate per piece
-    double tie;                       // guard on a rounding tie of the second query (s)
-    double ulp_q;                     // ulp of the absolute query time
+    // Read by the fast pass for every (sample, transmitter): the first 144
+    // bytes, in adjacent 16-byte pairs:
+    double p0[3];                     // first-iterate delay, piece 0 (unrounded query)
+    double p1[3];                     // second-iterate delay, piece 0
+    double k0, k1;                    // ∂delay/∂(query time): first iterate; second iterate, piece 0
+    double hm;                        // a second query's rounding offset below hm is not within the
+                                      // tie guard of a rounding midpoint: half its ulp less the guard
+                                      // (exact: both powers of two; the guard off gives half an ulp + 1)
     double tau_if;                    // 2π (f_tx - f_lo)
+    double nts;                       // -2π f_tx (the transmitter's)
     double guard;                     // emission-time guard band (s)
-    float amp0, amp1;                 // amplitude = amp0 + amp1 Δ
-    int32_t flags;
-    int32_t nav_pm;                   // nav sign of the tile (1 with nav off; unused with kRecNavVary)
-    int64_t sym_lo, sym_hi;           // framed kinds, one-shot frame: the symbols f0 + m of the frame
-                                      // are those with m in [sym_lo, sym_hi)
     double chip_base;                 // C/A and framed kinds: 1.5 x 2^52 - f0, f0 a whole chip / symbol
                                       // count at or below the tile's first one (floor(x) + chip_base
                                       // holds floor(x) - f0 in its low 32 bits, exactly)
+    double epoch_rel;                 // the transmitter's symbol / chip epoch (scene-epoch relative)
+    float amp0, amp1;                 // amplitude = amp0 + amp1 Δ
+    int32_t flags;
     int32_t chip_m0;                  // C/A: f0 mod 1023; framed kinds: the frame slot of count f0
                                       // (repeating frame) or f0 itself (one-shot frame)
+    int32_t nav_pm;                   // nav sign of the tile (1 with nav off; unused with kRecNavVary)
     int32_t n_nodes;                  // most grid nodes either iterate crosses in the tile
+    int32_t sym_lo, sym_hi;           // framed kinds, one-shot frame: the symbols f0 + m of the frame
+                                      // are those with m in [sym_lo, sym_hi)
+    // Read once per tile, or by the multi-piece passes only:
+    double tu0, tu_hi;                // fit range; Δ origin tu0
+    // An iterate's query crosses up to kSplitNodes grid nodes inside a tile
+    // (a tile up to 3 grid steps long): piece q >= 1 starts at the q-th node
+    // (absolute query time, kSplitInf when absent). Pieces 0-1 live here,
+    // pieces 2-3 of a tile with n_nodes > 1 in its AnchorExt.
+    double node0, node1;              // first node of each iterate
+    double p0b[3], p1b[3];            // piece 1 of each iterate
+    double k1b;                       // second-iterate slope of piece 1
+    double reserved;
 };
 static_assert(sizeof(AnchorRec) % 16 == 0, "AnchorRec arrays must keep 16-byte alignment");
+static_assert(offsetof(AnchorRec, tu0) == 144 && offsetof(AnchorRec, amp0) == 112,
+              "the fast pass's fields fill the record's first 144 bytes");
 
 // Pieces 2-3 of a tile whose iterates cross more than one grid node (low
 // sample rates): read from global memory by the multi-node pass only.
@@ -96,11 +110,13 @@ struct __align__(16) AnchorExt {
 
 // Lerp position at epoch-relative time t with the segment forced to `lo`
 // (linear extrapolation beyond it), without rounding epoch + t: de is
-// epoch - t0 of the grid, exact.
+// epoch - t0 of the grid, exact. The fraction scales by 1/dt: a smooth
+// function of t either way, which is all the fits and the converged solve
+// need (the reference's own query keeps its division, solve_reference).
 __device__ __forceinline__ void pos_unrounded(const DevTx &tx, double t, double de, int64_t lo, double &x,
                                               double &y, double &z) {
     if (tx.traj_kind == 0) { x = tx.sx; y = tx.sy; z = tx.sz; return; }
-    double frac = (t + de) / tx.dt - (double)lo;
+    double frac = (t + de) * tx.inv_dt - (double)lo;
     double4 a = load_point(tx.grid + lo), b = load_point(tx.grid + lo + 1);
     double omf = 1.0 - frac;
     x = a.x * omf + b.x * frac;
@@ -112,7 +128,7 @@ __device__ __forceinline__ void pos_unrounded(const DevTx &tx, double t, double 
 // reference's lerp would clamp there.
 __device__ __forceinline__ int64_t seg_unrounded(const DevTx &tx, double t, double de, bool &clamped) {
     if (tx.traj_kind == 0) { clamped = false; return 0; }
-    double f = (t + de) / tx.dt;
+    double f = (t + de) * tx.inv_dt;
     int64_t lo = floor_to_i64(f);
     clamped = lo < 0 || lo > tx.grid_n - 2;
     return lo < 0 ? 0 : (lo > tx.grid_n - 2 ? tx.grid_n - 2 : lo);
@@ -133,7 +149,7 @@ __device__ __forceinline__ double iterate_unrounded(const DevTx &tx, double tu, 
         double vx = 0.0, vy = 0.0, vz = 0.0;
         if (tx.traj_kind != 0) {
             double4 a = load_point(tx.grid + lo), b = load_point(tx.grid + lo + 1);
-            vx = (b.x - a.x) / tx.dt; vy = (b.y - a.y) / tx.dt; vz = (b.z - a.z) / tx.dt;
+            vx = (b.x - a.x) * tx.inv_dt; vy = (b.y - a.y) * tx.inv_dt; vz = (b.z - a.z) * tx.inv_dt;
         }
         *dd_dt = ((dx * (vx + w * vy) + dy * (vy - w * vx) + dz * vz) / r) * inv_c;
     }
@@ -149,11 +165,11 @@ __device__ __forceinline__ void store_recs(const AnchorRec *__restrict__ s, Anch
     for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
 }
 
-// Newton form of the quadratic through (0, v0), (h, v1), (2h, v2).
-__device__ __forceinline__ void quad3(double v0, double v1, double v2, double h, double c[3]) {
+// Newton form of the quadratic through (0, v0), (h, v1), (2h, v2); ih = 1/h.
+__device__ __forceinline__ void quad3(double v0, double v1, double v2, double h, double ih, double c[3]) {
     if (!(h > 0.0)) { c[0] = v0; c[1] = 0.0; c[2] = 0.0; return; }
-    double s1 = (v1 - v0) / h, s2 = (v2 - v1) / h;
-    c[2] = (s2 - s1) / (2.0 * h);
+    double s1 = (v1 - v0) * ih, s2 = (v2 - v1) * ih;
+    c[2] = (s2 - s1) * (0.5 * ih);
     c[1] = s1 - c[2] * h;
     c[0] = v0;
 }
@@ -193,6 +209,7 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
     const double tus = tls - (b.clock_offset + b.clock_y0 * tls) - kSplitMargin;
     const double h = 0.5 * ((tle - (b.clock_offset + b.clock_y0 * tle) + kSplitMargin) - tus);
     const double tue = tus + 2.0 * h;  // the third fit time, exactly
+    const double ih = h > 0.0 ? 1.0 / h : 0.0;
     const double ox = b.rx[0], oy = b.rx[1], oz = b.rx[2];
     const double de = tx.traj_kind != 0 ? b.epoch - tx.t0 : 0.0;
     r.tu0 = tus;
@@ -202,16 +219,16 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
     r.tau_if = kTau * (tx.carrier - b.lo);
     r.flags = 0;
     r.nav_pm = 1;
-    r.k0 = 0.0;
-    for (int p = 0; p < 2; ++p) {
-        r.k1[p] = 0.0;
-        for (int i = 0; i < 3; ++i) r.p0[p][i] = r.p1[p][i] = 0.0;
-    }
+    r.k0 = r.k1 = r.k1b = 0.0;
+    for (int i = 0; i < 3; ++i) r.p0[i] = r.p1[i] = r.p0b[i] = r.p1b[i] = 0.0;
     r.chip_base = 0.0;
     r.chip_m0 = 0;
+    r.nts = tx.neg_tau_src;
+    r.epoch_rel = tx.epoch_rel;
+    r.reserved = 0.0;
     if (exact_only) {
         r.amp0 = r.amp1 = 0.0f;
-        r.guard = r.ulp_q = r.tie = 0.0;
+        r.guard = r.hm = 0.0;
         r.sym_lo = r.sym_hi = 0;
         r.flags = kRecExact;
         return;
@@ -261,7 +278,7 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
                 v[i] = l0[0] + p == l0[i] ? d0[i]
                                           : iterate_unrounded(tx, tu[i], tu[i] - kEmissionLag, de, l0[0] + p, ox, oy,
                                                               oz, b.inv_c, nullptr, nullptr);
-            quad3(v[0], v[1], v[2], h, p < 2 ? r.p0[p] : x->p0[p - 2]);
+            quad3(v[0], v[1], v[2], h, ih, p == 0 ? r.p0 : (p == 1 ? r.p0b : x->p0[p - 2]));
         }
         for (int64_t p = 0; p <= n1; ++p) {
             double k1 = 0.0;
@@ -272,11 +289,11 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
                                          i == 1 ? &k1 : nullptr);
             }
             if (l1[0] + p == l1[1]) d1m = v[1];  // the second iterate on its natural segment at the middle
-            if (p < 2) r.k1[p] = k1; else x->k1[p - 2] = k1;
-            quad3(v[0], v[1], v[2], h, p < 2 ? r.p1[p] : x->p1[p - 2]);
+            if (p == 0) r.k1 = k1; else if (p == 1) r.k1b = k1; else x->k1[p - 2] = k1;
+            quad3(v[0], v[1], v[2], h, ih, p == 0 ? r.p1 : (p == 1 ? r.p1b : x->p1[p - 2]));
         }
-        te_s = tus - poly2(r.p1[0], 0.0);
-        te_e = tue - poly2(n1 < 2 ? r.p1[n1] : x->p1[n1 - 2], 2.0 * h);
+        te_s = tus - poly2(r.p1, 0.0);
+        te_e = tue - poly2(n1 == 0 ? r.p1 : (n1 == 1 ? r.p1b : x->p1[n1 - 2]), 2.0 * h);
     }
     float amp_s = (float)(tx.amp_factor / rs), amp_e = (float)(tx.amp_factor / re);
     if (!exact && b.has_antenna) {
@@ -307,9 +324,12 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
     // reference's by a few ulp of t1, so a sum within `tie` of a rounding
     // midpoint takes the exact path. When ulp_q is that fine the rounding is
     // immaterial (< 1e-19 s of delay) and the check is off (tie < 0).
-    r.ulp_q = ldexp(1.0, ilogb(fmax(fmax(fabs(b.epoch + tus), fabs(b.epoch + tue)), 1e-300)) - 52);
+    const double ulp_q = ldexp(1.0, ilogb(fmax(fmax(fabs(b.epoch + tus), fabs(b.epoch + tue)), 1e-300)) - 52);
     const double tie = ldexp(8.0, ilogb(fmax(fmax(fabs(tus), fabs(tue)), 1.0)) - 52);
-    r.tie = (8.0 * tie > r.ulp_q) ? -1.0 : tie;
+    // A rounding error never exceeds half an ulp, so "|(|err| - half)| > tie"
+    // (not within `tie` of a tie) is |err| < half - tie; half and tie are
+    // powers of two, so the difference is exact (guard off: always true)
+    r.hm = 0.5 * ulp_q - ((8.0 * tie > ulp_q) ? -1.0 : tie);
     r.sym_lo = 0;
     r.sym_hi = 0;
     if (!exact && (tx.sig_kind == kBpsk || tx.sig_kind == kOok || tx.sig_kind == kQam16)) {
@@ -334,8 +354,8 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
                 if (!(xe - f0 + 2.0 < (double)tx.n_sym)) exact = true;
             } else {  // f0 within [-2^30, n_sym) here, so every count below fits 32 bits
                 r.chip_m0 = (int32_t)f0i;
-                r.sym_lo = -f0i;
-                r.sym_hi = tx.n_sym - f0i;
+                r.sym_lo = (int32_t)(-f0i);
+                r.sym_hi = (int32_t)(tx.n_sym - f0i);
             }
         }
     }
@@ -433,7 +453,7 @@ __device__ __forceinline__ void split_baseband(const DevTx &tx, const AnchorRec 
                                                float &bre, float &bim) {
     bim = 0.0f;
     if constexpr (K == kPassCa || K == kPassCaNav) {  // ca_code.rs:167-193
-        const double dt = __dsub_rn(te, tx.epoch_rel);
+        const double dt = __dsub_rn(te, R.epoch_rel);
         const double cp = __dmul_rn(dt, kCaChipRate);
         const double fl = floor(cp), fr = cp - fl, g = guard * kCaChipRate;
         ok &= fr >= g && fr <= 1.0 - g;
@@ -460,7 +480,7 @@ __device__ __forceinline__ void split_baseband(const DevTx &tx, const AnchorRec 
         const int chip = ((tx.chip_neg[m >> 5] >> (m & 31)) & 1u) ? -nav : nav;
         bre = (float)chip;
     } else if constexpr (K == kPassBpsk || K == kPassOok || K == kPassQam) {  // frame_index, signal/mod.rs:109-115
-        const double f = __dmul_rn(__dsub_rn(te, tx.epoch_rel), tx.rate);
+        const double f = __dmul_rn(__dsub_rn(te, R.epoch_rel), tx.rate);
         const double fl = floor(f), fr = f - fl, g = guard * tx.rate;
         ok &= fr >= g && fr <= 1.0 - g;
         // m = floor(f) - f0, read from the low word of an exact add (the
@@ -511,17 +531,15 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
                                            unsigned fit, float *ar, float *ai, unsigned &redo, int64_t first,
                                            double *dbg_phase, double *dbg_temit, double *dbg_delay,
                                            const DevBand *acc_band = nullptr, double *acc = nullptr) {
-    const double k0 = R.k0;
-    // A rounding error never exceeds half an ulp, so "|(|err| - half)| > tie"
-    // (not within `tie` of a tie) is |err| < half - tie; half and tie are
-    // powers of two, so the difference is exact (tie < 0: always true).
-    const double hm = 0.5 * R.ulp_q - R.tie;
-    const double tau_if = R.tau_if, nts = tx.neg_tau_src, guard = R.guard;
+    // the record's first 144 bytes hold everything read here, in adjacent
+    // 16-byte pairs; read from shared memory where used, so the compiler can
+    // re-read a value instead of spilling it
+    const double k0 = R.k0, hm = R.hm, tau_if = R.tau_if, nts = R.nts, guard = R.guard;
     const float amp0 = R.amp0, amp1 = R.amp1;
     // one piece per iterate (no grid node inside the tile): coefficients in registers
-    const double a0 = R.p0[0][0], a1 = R.p0[0][1], a2 = R.p0[0][2];
-    const double b0 = R.p1[0][0], b1 = R.p1[0][1], b2 = R.p1[0][2];
-    const double ka = R.k1[0];
+    const double a0 = R.p0[0], a1 = R.p0[1], a2 = R.p0[2];
+    const double b0 = R.p1[0], b1 = R.p1[1], b2 = R.p1[2];
+    const double ka = R.k1;
 #pragma unroll
     for (int s = 0; s < S; ++s) {
         const SampleCtx &c = sc[s];
@@ -530,7 +548,7 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
         if constexpr (NK > 0) {
             const double q = __dadd_rn(epoch, __dsub_rn(tu, kEmissionLag));
             const int i0 = q >= R.node0;
-            const double *p0 = R.p0[i0];
+            const double *p0 = i0 ? R.p0b : R.p0;
             if constexpr (NK > 1) {
                 const int j0 = (q >= X->node0[0]) + (q >= X->node0[1]);
                 if (j0 > 0) p0 = X->p0[j0 - 1];
@@ -545,8 +563,8 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
         bool ok = fabs(e1 - t1r) < hm;
         if constexpr (NK > 0) {
             const int i1 = s1 >= R.node1;
-            const double *p1 = R.p1[i1];
-            double kk = R.k1[i1];
+            const double *p1 = i1 ? R.p1b : R.p1;
+            double kk = i1 ? R.k1b : R.k1;
             if constexpr (NK > 1) {
                 const int j1 = (s1 >= X->node1[0]) + (s1 >= X->node1[1]);
                 if (j1 > 0) {
