@@ -7,12 +7,14 @@
 // (-ffp-contract=off), as the reference's Rust code does on x86_64 Linux,
 // so trajectory grids and signal tables are bit-identical to its own.
 #include <algorithm>
+#include <atomic>
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/lipika_cuda.h"
@@ -382,6 +384,7 @@ lpk_status build_tx(const lpk_transmitter_cfg &c, const lpk_scene_cfg &scene, Tx
             return host_fail(LPK_EINVAL, "bad payload / sync word");
         Xoshiro rng(c.payload_seed);
         if (c.kind == LPK_SIG_BPSK) {  // BpskFrame::random (bpsk.rs:28-42)
+            h.pm.reserve((size_t)c.sync_n + (size_t)c.payload_n);
             h.pm.assign(c.sync_word, c.sync_word + c.sync_n);
             for (int64_t i = 0; i < c.payload_n; ++i) h.pm.push_back(rng.bool_half() ? 1 : -1);
             d.n_sym = (int64_t)h.pm.size();
@@ -390,6 +393,7 @@ lpk_status build_tx(const lpk_transmitter_cfg &c, const lpk_scene_cfg &scene, Tx
             for (int i = 0; i < c.sync_n; ++i)
                 if (c.sync_word[i] < 0 || c.sync_word[i] > 1)
                     return host_fail(LPK_EINVAL, "ook sync_word entries must be 0 or 1");
+            h.ook.reserve((size_t)c.sync_n + (size_t)c.payload_n);
             for (int i = 0; i < c.sync_n; ++i) h.ook.push_back((uint8_t)c.sync_word[i]);
             for (int64_t i = 0; i < c.payload_n; ++i) h.ook.push_back((uint8_t)rng.bool_half());
             d.n_sym = (int64_t)h.ook.size();
@@ -400,14 +404,15 @@ lpk_status build_tx(const lpk_transmitter_cfg &c, const lpk_scene_cfg &scene, Tx
                     return host_fail(LPK_EINVAL, "qam16 sync_word entries must be 0 or 1");
             if (c.sync_n % 4) return host_fail(LPK_EINVAL, "qam16 sync_word must hold whole symbols");
             const float scale = 0.31622777f;
+            h.sym.reserve((size_t)(c.sync_n / 4) + (size_t)c.payload_n);
             for (int i = 0; i < c.sync_n; i += 4) {
                 const int8_t *b = c.sync_word + i;
                 h.sym.push_back({gray((uint8_t)b[0], (uint8_t)b[1]) * scale, gray((uint8_t)b[2], (uint8_t)b[3]) * scale});
             }
-            for (int64_t i = 0; i < c.payload_n; ++i) {
-                uint32_t v = rng.range16();
-                h.sym.push_back({gray((v >> 3) & 1, (v >> 2) & 1) * scale, gray((v >> 1) & 1, v & 1) * scale});
-            }
+            lpk_cf32 point[16];  // map_symbol (qam16.rs:32-34) of each 4-bit value, same f32 products
+            for (uint32_t v = 0; v < 16; ++v)
+                point[v] = {gray((v >> 3) & 1, (v >> 2) & 1) * scale, gray((v >> 1) & 1, v & 1) * scale};
+            for (int64_t i = 0; i < c.payload_n; ++i) h.sym.push_back(point[rng.range16()]);
             d.n_sym = (int64_t)h.sym.size();
             d.symbols = h.sym.data();
         }
@@ -503,9 +508,29 @@ lpk_status lpk_scene_prepare(lpk_ctx *ctx, const lpk_scene_cfg *cfg, lpk_scene *
     const bool device_grid = (cfg->flags & LPK_SCENE_DEVICE_TABLES) != 0;
     if (device_grid && !ctx) return host_fail(LPK_EINVAL, "LPK_SCENE_DEVICE_TABLES needs a context");
     s->tx.resize((size_t)cfg->n_transmitters);
-    for (int32_t i = 0; i < cfg->n_transmitters; ++i) {
-        lpk_status st = build_tx(cfg->transmitters[i], *cfg, s->tx[i], device_grid);
-        if (st) return st;
+    {
+        // Transmitters are independent (their tables depend only on their own
+        // config): built on the host's threads. On failure the lowest failing
+        // index is rebuilt alone, so its status and message are reported as a
+        // sequential build would report them.
+        const int32_t n_tx = cfg->n_transmitters;
+        std::vector<lpk_status> status((size_t)n_tx, LPK_OK);
+        std::atomic<int32_t> next{0};
+        auto work = [&]() {
+            for (int32_t i = next++; i < n_tx; i = next++)
+                status[(size_t)i] = build_tx(cfg->transmitters[i], *cfg, s->tx[i], device_grid);
+        };
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const int32_t nt = (int32_t)std::min<unsigned>(hw, (unsigned)std::max(n_tx, 0));
+        std::vector<std::thread> pool;
+        for (int32_t k = 1; k < nt; ++k) pool.emplace_back(work);
+        work();
+        for (auto &t : pool) t.join();
+        for (int32_t i = 0; i < n_tx; ++i)
+            if (status[(size_t)i] != LPK_OK) {
+                s->tx[i] = TxHost();
+                return build_tx(cfg->transmitters[i], *cfg, s->tx[i], device_grid);
+            }
     }
     if (device_grid) {  // every pending grid shares the scene's start, step and length
         std::vector<lpk_kepler_orbit> orbits;
