@@ -196,6 +196,16 @@ typedef struct lpk_band_desc {
     int32_t n_post;
     int32_t solver;             /* LPK_SOLVER_* */
     lpk_post_op post[3];
+    /* Flicker-FM part of the clock (Flicker, src/clock/mod.rs:55-149) for
+     * the DETERMINISTIC and DEVICE_WALK modes: the coarse flicker track D[m]
+     * at m / 128 s of local time, m = 0..flicker_n-1, in HOST memory
+     * (lpk_clock_flicker_table; the host stream interpolates it linearly,
+     * Flicker::delta_at, :142-148, and so do the kernels). NULL: no
+     * flicker. Ignored under LPK_CLOCK_HOST, whose Δt already holds it.
+     * lpk_scene_band_desc fills it for a clock with a flicker floor; the
+     * scene owns that table. */
+    const double *flicker_delta_s;
+    int64_t flicker_n;
 } lpk_band_desc;
 
 /* One chunk of one band through the fan-out, Σ, AWGN and rx chain.
@@ -533,6 +543,18 @@ lpk_status lpk_generate_scene(lpk_scene *s, uint64_t seed_base, double round_s, 
  * the caller, which holds the band metadata. */
 lpk_status lpk_generate_scene_to_files(lpk_scene *s, uint64_t seed_base, double round_s, int32_t flags,
                                        const char *const *paths);
+
+/* The flicker track of a receiver clock with a flicker floor, for the
+ * device clock modes (lpk_band_desc.flicker_delta_s): out[m] = the flicker
+ * Δt at m / 128 s after the band start, m = 0..n-1, the values the host
+ * clock stream with the same spec and seed interpolates between
+ * (Flicker::new and advance_to, src/clock/mod.rs:95-140; calibrated and
+ * warmed on its own long-jumped copies of the clock's generator, so it does
+ * not depend on the white-FM draws). seed: clock_seed(base, r_idx),
+ * src/pipeline.rs:825-827. lpk_clock_flicker_len(duration_s) points cover a
+ * band of duration_s. LPK_EINVAL for a spec without a flicker floor. */
+int64_t lpk_clock_flicker_len(double duration_s);
+lpk_status lpk_clock_flicker_table(const lpk_clock_cfg *spec, uint64_t seed, double *out, int64_t n);
 
 /* Host clock stream (ClockStream, src/clock/mod.rs:229-347) exposed for
  * tests: delta_t_at over n monotone times. */

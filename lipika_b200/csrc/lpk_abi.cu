@@ -96,6 +96,8 @@ lpk_status build_dev_band(lpk_ctx *ctx, const lpk_band_desc *d, int64_t i0, int6
         (!(d->clock_master_rate_hz > 0.0) || !finite(d->clock_master_rate_hz) || !(d->clock_allan_1s >= 0.0) ||
          !finite(d->clock_allan_1s)))
         return fail(ctx, LPK_EINVAL, "device clock walk needs a positive master rate and allan >= 0");
+    if (d->flicker_delta_s && d->clock_mode != LPK_CLOCK_HOST && d->flicker_n < 2)
+        return fail(ctx, LPK_EINVAL, "flicker track needs at least two points");
     if (d->n_post < 0 || d->n_post > 3) return fail(ctx, LPK_EINVAL, "n_post must be 0..3");
     if (d->solver != LPK_SOLVER_REFERENCE && d->solver != LPK_SOLVER_SPLIT && d->solver != LPK_SOLVER_FP64_TUNED)
         return fail(ctx, LPK_EINVAL, "unknown solver");
@@ -218,6 +220,67 @@ lpk_status prepare_walk(lpk_ctx *c, const lpk_band_desc *d, int64_t i0, int64_t 
     b.eps = d_eps;
     b.eps_k0 = kA;
     b.fm = d->clock_master_rate_hz;
+    return LPK_OK;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Coarse flicker points [m_lo, m_lo + count) that band samples [i0, i0 + n)
+// read (band_flicker: points floor(t·128) and floor(t·128) + 1), with one
+// point of margin on either side, clamped to the track; -1 when the track
+// does not reach the chunk's last sample.
+static int64_t flicker_span(const lpk_band_desc *d, int64_t i0, int64_t n, int64_t *m_lo) {
+    const double fs = d->fs_hz;
+    const double x0 = ((double)i0 / fs) * kFlickerRate;
+    const double x1 = ((double)(i0 + (n > 0 ? n - 1 : 0)) / fs) * kFlickerRate;
+    const int64_t a = x0 <= 0.0 ? 0 : (int64_t)std::floor(x0);
+    const int64_t need = (x1 <= 0.0 ? 0 : (int64_t)std::floor(x1)) + 1;
+    if (need >= d->flicker_n) return -1;
+    const int64_t lo = a > 0 ? a - 1 : 0, hi = need + 1 < d->flicker_n ? need + 1 : need;
+    *m_lo = lo;
+    return hi - lo + 1;
+}
+
+static bool uses_flicker(const lpk_band_desc *d) {
+    return d->flicker_delta_s && d->clock_mode != LPK_CLOCK_HOST;
+}
+
+size_t clock_region_bytes(const lpk_band_desc *d, int64_t i0, int64_t n) {
+    size_t bytes = 0;
+    int64_t k = 0;
+    if (d->clock_mode == LPK_CLOCK_DEVICE_WALK) bytes += align256(sizeof(double) * (size_t)walk_span(d, i0, n, &k));
+    if (uses_flicker(d)) {
+        const int64_t cnt = flicker_span(d, i0, n, &k);  // -1 (a short track): prepare_clock refuses it
+        bytes += align256(sizeof(double) * (size_t)(cnt > 0 ? cnt : 1));
+    }
+    return bytes;
+}
+
+lpk_status prepare_clock(lpk_ctx *c, const lpk_band_desc *d, int64_t i0, int64_t n, DevBand &b, char *region) {
+    size_t off = 0;
+    int64_t k = 0;
+    if (d->clock_mode == LPK_CLOCK_DEVICE_WALK) {
+        const int64_t span = walk_span(d, i0, n, &k);
+        lpk_status st = prepare_walk(c, d, i0, n, b, (double *)region, span);
+        if (st) return st;
+        off = align256(sizeof(double) * (size_t)span);
+    }
+    return stage_flicker(c, d, i0, n, b, (double *)(region + off), INT64_MAX);
+}
+
+lpk_status stage_flicker(lpk_ctx *c, const lpk_band_desc *d, int64_t i0, int64_t n, DevBand &b, double *dst,
+                         int64_t cap) {
+    if (!uses_flicker(d)) return LPK_OK;
+    int64_t m_lo = 0;
+    const int64_t cnt = flicker_span(d, i0, n, &m_lo);
+    if (cnt < 2) return fail(c, LPK_EINVAL, "flicker track shorter than the chunk");
+    if (cnt > cap) return fail(c, LPK_EINVAL, "chunk spans more flicker points than its scratch holds");
+    cudaError_t e = cudaMemcpyAsync(dst, d->flicker_delta_s + m_lo, sizeof(double) * (size_t)cnt,
+                                    cudaMemcpyHostToDevice, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "flicker track upload");
+    b.flicker = dst;
+    b.flicker_m0 = m_lo;
+    b.flicker_n = cnt;
     return LPK_OK;
 }
 
@@ -576,8 +639,6 @@ lpk_status lpk_scene_upload(lpk_ctx *c, const lpk_tx_desc *tx, int32_t n_tx) {
     return LPK_OK;
 }
 
-static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
-
 // Split path of a chunk entry point: the anchor fits on the side stream
 // (after everything already queued on the context's stream, so the previous
 // chunk's fan-out has read its records), the walk on the main stream, then
@@ -608,9 +669,9 @@ lpk_status lpk_band_chunk_device(lpk_ctx *c, const lpk_band_desc *band, const in
     // active list, unoccluded words and the clock walk live in the scratch
     size_t off_uw = align256(sizeof(int32_t) * 256);
     size_t off_eps = off_uw + align256(sizeof(uint32_t) * 256);
-    int64_t kA = 0, span = b.clock_mode == LPK_CLOCK_DEVICE_WALK ? walk_span(band, i0, n, &kA) : 0;
+    const size_t clk_bytes = clock_region_bytes(band, i0, n);
     const bool split = use_split(band);
-    size_t off_recs = off_eps + align256(sizeof(double) * (size_t)span);
+    size_t off_recs = off_eps + clk_bytes;
     size_t recs = split ? align256(split_recs_bytes(c->split_variant, i0, n, n_active)) : 0;
     if ((st = ensure_scratch(c, off_recs + recs))) return st;
     int32_t *d_active = (int32_t *)c->d_scratch;
@@ -621,7 +682,7 @@ lpk_status lpk_band_chunk_device(lpk_ctx *c, const lpk_band_desc *band, const in
     if (e != cudaSuccess) return cuda_fail(c, e, "chunk setup");
     if (split && (e = split_fork_anchor(c, b, d_active, n_active, (char *)c->d_scratch + off_recs)) != cudaSuccess)
         return cuda_fail(c, e, "anchor fits");
-    if (span && (st = prepare_walk(c, band, i0, n, b, (double *)((char *)c->d_scratch + off_eps), span))) return st;
+    if (clk_bytes && (st = prepare_clock(c, band, i0, n, b, (char *)((char *)c->d_scratch + off_eps)))) return st;
     if (split && (e = cudaStreamWaitEvent(c->stream, c->ev_join, 0)) != cudaSuccess) return cuda_fail(c, e, "join");
     prof_begin(c);
     if (split) {
@@ -662,8 +723,8 @@ lpk_status lpk_split_accuracy(lpk_ctx *c, const lpk_band_desc *band, const int32
     const size_t off_stats = align256(sizeof(int32_t) * 256);
     const size_t off_out = off_stats + 256;
     const size_t off_eps = off_out + (d_out ? 0 : align256(sizeof(float2) * (size_t)(n > 0 ? n : 0)));
-    int64_t kA = 0, span = b.clock_mode == LPK_CLOCK_DEVICE_WALK ? walk_span(band, i0, n, &kA) : 0;
-    const size_t off_recs = off_eps + align256(sizeof(double) * (size_t)span);
+    const size_t clk_bytes = clock_region_bytes(band, i0, n);
+    const size_t off_recs = off_eps + clk_bytes;
     if ((st = ensure_scratch(c, off_recs + align256(split_recs_bytes(c->split_variant, i0, n, n_active)))))
         return st;
     char *base = (char *)c->d_scratch;
@@ -676,7 +737,7 @@ lpk_status lpk_split_accuracy(lpk_ctx *c, const lpk_band_desc *band, const int32
     if (e != cudaSuccess) return cuda_fail(c, e, "accuracy setup");
     if ((e = split_fork_anchor(c, b, d_active, n_active, base + off_recs)) != cudaSuccess)
         return cuda_fail(c, e, "anchor fits");
-    if (span && (st = prepare_walk(c, band, i0, n, b, (double *)(base + off_eps), span))) return st;
+    if (clk_bytes && (st = prepare_clock(c, band, i0, n, b, (char *)(base + off_eps)))) return st;
     if ((e = cudaStreamWaitEvent(c->stream, c->ev_join, 0)) != cudaSuccess) return cuda_fail(c, e, "join");
     b.acc_stats = d_stats;
     e = launch_split_fanout(c->split_variant, b, c->d_tx, d_active, n_active, base + off_recs, out, nullptr, nullptr,
@@ -724,9 +785,9 @@ lpk_status lpk_band_chunk(lpk_ctx *c, const lpk_band_desc *band, const int32_t *
     size_t n_rx = b.rx_kind == LPK_RX_PER_SAMPLE ? 3 * (size_t)n : 0;
     size_t off_out = off_rx + align256(sizeof(double) * n_rx);
     size_t off_eps = off_out + align256(sizeof(float2) * (size_t)n);
-    int64_t kA = 0, span = b.clock_mode == LPK_CLOCK_DEVICE_WALK ? walk_span(band, i0, n, &kA) : 0;
+    const size_t clk_bytes = clock_region_bytes(band, i0, n);
     const bool split = use_split(band);
-    size_t off_recs = off_eps + align256(sizeof(double) * (size_t)span);
+    size_t off_recs = off_eps + clk_bytes;
     size_t total = off_recs + (split ? align256(split_recs_bytes(c->split_variant, i0, n, n_active)) : 0);
     if ((st = ensure_scratch(c, total))) return st;
     char *base = (char *)c->d_scratch;
@@ -747,7 +808,7 @@ lpk_status lpk_band_chunk(lpk_ctx *c, const lpk_band_desc *band, const int32_t *
     b.rxpos = d_rx;
     if (split && (e = split_fork_anchor(c, b, d_active, n_active, base + off_recs)) != cudaSuccess)
         return cuda_fail(c, e, "anchor fits");
-    if (span && (st = prepare_walk(c, band, i0, n, b, (double *)(base + off_eps), span))) return st;
+    if (clk_bytes && (st = prepare_clock(c, band, i0, n, b, (char *)(base + off_eps)))) return st;
     if (split && (e = cudaStreamWaitEvent(c->stream, c->ev_join, 0)) != cudaSuccess) return cuda_fail(c, e, "join");
     prof_begin(c);
     if (split) {
@@ -813,10 +874,10 @@ lpk_status lpk_tx_contribution(lpk_ctx *c, const lpk_band_desc *band, int32_t tx
     cudaSetDevice(c->device);
     size_t bytes = sizeof(double) * (size_t)n;
     const bool split = use_split(band);
-    int64_t kA = 0, span = b.clock_mode == LPK_CLOCK_DEVICE_WALK ? walk_span(band, i0, n, &kA) : 0;
+    const size_t clk_bytes = clock_region_bytes(band, i0, n);
     size_t off_act = 8 * bytes;
     size_t off_eps = off_act + 256;
-    size_t off_recs = off_eps + align256(sizeof(double) * (size_t)span);
+    size_t off_recs = off_eps + clk_bytes;
     const size_t recs_bytes = split ? align256(split_recs_bytes(c->split_variant, i0, n, 1)) : 0;
     lpk_status s2 = ensure_scratch(c, off_recs + recs_bytes + 256);
     if (s2) return s2;
@@ -835,7 +896,7 @@ lpk_status lpk_tx_contribution(lpk_ctx *c, const lpk_band_desc *band, int32_t tx
     if (e != cudaSuccess) return cuda_fail(c, e, "transmitter contribution upload");
     b.delta = d_delta;
     b.rxpos = d_rx;
-    if (span && (s2 = prepare_walk(c, band, i0, n, b, (double *)(base + off_eps), span))) return s2;
+    if (clk_bytes && (s2 = prepare_clock(c, band, i0, n, b, (char *)(base + off_eps)))) return s2;
     if (split) {
         b.has_noise = 0;  // the contribution alone, as transmitter_contribution_at_receiver returns it
         b.n_post = 0;
@@ -883,11 +944,11 @@ lpk_status lpk_clock_device_delta(lpk_ctx *c, const lpk_band_desc *band, int64_t
     if (n == 0) return LPK_OK;
     if (!out) return fail(c, LPK_EINVAL, "delta_out is NULL");
     cudaSetDevice(c->device);
-    int64_t kA = 0, span = b.clock_mode == LPK_CLOCK_DEVICE_WALK ? walk_span(band, i0, n, &kA) : 0;
+    const size_t clk_bytes = clock_region_bytes(band, i0, n);
     size_t off_eps = align256(sizeof(double) * (size_t)n);
-    if ((st = ensure_scratch(c, off_eps + align256(sizeof(double) * (size_t)span)))) return st;
+    if ((st = ensure_scratch(c, off_eps + clk_bytes))) return st;
     double *d_out = (double *)c->d_scratch;
-    if (span && (st = prepare_walk(c, band, i0, n, b, (double *)((char *)c->d_scratch + off_eps), span))) return st;
+    if (clk_bytes && (st = prepare_clock(c, band, i0, n, b, (char *)((char *)c->d_scratch + off_eps)))) return st;
     cudaError_t e = launch_band_delta(b, d_out, c->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(out, d_out, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, c->stream);

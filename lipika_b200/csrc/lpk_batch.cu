@@ -659,6 +659,24 @@ lpk_status lpk_batch_create(lpk_ctx *c, const lpk_work_unit *wu, int32_t n_units
         if (!st) st = batch_alloc(b, &p, sizeof(double) * (size_t)(total_blocks[w] / kGroupBlocks + 1)),
                  h_walks[w].gsum = (double *)p;
     }
+    for (int u = 0; u < n_units && !st; ++u) {  // flicker tracks: each unit's whole track, uploaded once
+        const lpk_band_desc &d = b->units[u].desc;
+        if (!d.flicker_delta_s) continue;
+        const int64_t last = b->units[u].n_samples > 0 ? b->units[u].n_samples - 1 : 0;
+        const double x = ((double)last / d.fs_hz) * kFlickerRate;
+        if ((x > 0.0 ? (int64_t)std::floor(x) : 0) + 1 >= d.flicker_n) {
+            st = fail(c, LPK_EINVAL, "flicker track shorter than the work unit");
+            break;
+        }
+        st = batch_alloc(b, &p, sizeof(double) * (size_t)d.flicker_n);
+        if (st) break;
+        cudaError_t e = cudaMemcpyAsync(p, d.flicker_delta_s, sizeof(double) * (size_t)d.flicker_n,
+                                        cudaMemcpyHostToDevice, c->stream);
+        if (e != cudaSuccess) st = cuda_fail(c, e, "flicker track upload");
+        h_bands[u].flicker = (const double *)p;
+        h_bands[u].flicker_m0 = 0;
+        h_bands[u].flicker_n = d.flicker_n;
+    }
     if (!st && c->batch_kit) {  // streams, events and pinned descriptors of the last batch
         BatchKit *k = c->batch_kit;
         c->batch_kit = nullptr;

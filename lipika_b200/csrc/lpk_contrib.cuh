@@ -9,15 +9,30 @@
 
 namespace lpk {
 
+// Flicker::delta_at (clock/mod.rs:142-148) on the coarse track: the
+// host stream's interpolation, operation for operation. The index is
+// clamped to the staged points (a chunk stages every point its samples read).
+__device__ __forceinline__ double band_flicker(const DevBand &b, double elapsed) {
+    if (!b.flicker) return 0.0;
+    const double x = __dmul_rn(elapsed > 0.0 ? elapsed : 0.0, kFlickerRate);
+    const double fl = floor(x);
+    int64_t m = (int64_t)fl - b.flicker_m0;
+    m = m < 0 ? 0 : (m > b.flicker_n - 2 ? b.flicker_n - 2 : m);
+    const double frac = __dsub_rn(x, fl);
+    return __dadd_rn(__dmul_rn(b.flicker[m], __dsub_rn(1.0, frac)), __dmul_rn(b.flicker[m + 1], frac));
+}
+
 __device__ __forceinline__ double band_delta(const DevBand &b, int64_t j, double t_local) {
-    if (b.clock_mode == LPK_CLOCK_DETERMINISTIC)  // (ε=0 + flicker=0) + c + m·t, clock/mod.rs:311-345
-        return __dadd_rn(0.0, __dadd_rn(b.clock_offset, __dmul_rn(b.clock_y0, t_local)));
+    if (b.clock_mode == LPK_CLOCK_DETERMINISTIC)  // (ε=0 + flicker) + c + m·t, clock/mod.rs:311-345
+        return __dadd_rn(__dadd_rn(0.0, band_flicker(b, t_local)),
+                         __dadd_rn(b.clock_offset, __dmul_rn(b.clock_y0, t_local)));
     if (b.clock_mode == LPK_CLOCK_DEVICE_WALK) {  // ClockStream::delta_t_at, clock/mod.rs:329-346
         double x = __dmul_rn(t_local, b.fm);      // elapsed = t - 0.0
         if (x <= 0.0) {
             double e0 = b.eps[0 - b.eps_k0];
             if (b.eps_carry) e0 = __dadd_rn(b.eps_carry[0], e0);
-            return __dadd_rn(__dadd_rn(e0, 0.0), __dadd_rn(b.clock_offset, __dmul_rn(b.clock_y0, 0.0)));
+            return __dadd_rn(__dadd_rn(e0, band_flicker(b, 0.0)),
+                             __dadd_rn(b.clock_offset, __dmul_rn(b.clock_y0, 0.0)));
         }
         int64_t k0 = floor_to_i64(x);
         double frac = __dsub_rn(x, (double)k0);
@@ -27,7 +42,8 @@ __device__ __forceinline__ double band_delta(const DevBand &b, int64_t j, double
             hi = __dadd_rn(b.eps_carry[(k0 + 1) / kWalkBlock], hi);
         }
         double eps = __dadd_rn(__dmul_rn(lo, __dsub_rn(1.0, frac)), __dmul_rn(hi, frac));
-        return __dadd_rn(__dadd_rn(eps, 0.0), __dadd_rn(b.clock_offset, __dmul_rn(b.clock_y0, t_local)));
+        return __dadd_rn(__dadd_rn(eps, band_flicker(b, t_local)),
+                         __dadd_rn(b.clock_offset, __dmul_rn(b.clock_y0, t_local)));
     }
     return b.delta[j];
 }

@@ -21,6 +21,7 @@ constexpr double kEmissionLag = 0.07;                  // src/channel/mod.rs:23
 constexpr double kEarthRate = 7.2921151467e-5;         // src/channel/mod.rs:27
 constexpr double kCaChipRate = 1023000.0;              // src/signal/ca_code.rs:23
 constexpr double kNavBitRate = 50.0;                   // src/signal/ca_code.rs:27
+constexpr double kFlickerRate = 128.0;                 // src/clock/mod.rs:67 (flicker track rate)
 
 enum SigKind : int32_t { kCw = 0, kBpsk = 1, kOok = 2, kQam16 = 3, kCa = 4 };
 enum NavKind : int32_t { kNavOff = 0, kNavDummy = 1, kNavFull = 2 };
@@ -69,6 +70,9 @@ struct DevBand {
                                         // ε(k) = eps_carry[b] ⊕ P_b(k), b the scan block of k
     int64_t eps_k0;
     double fm;                          // master (walk) rate
+    const double *flicker;              // coarse flicker track points [flicker_m0, flicker_m0 + flicker_n)
+                                        // (DETERMINISTIC / DEVICE_WALK; NULL: no flicker)
+    int64_t flicker_m0, flicker_n;
     float noise_std;                    // sqrt(P/2) as f32; 0 = no noise
     int32_t has_noise;
     uint64_t noise_seed;

@@ -12,7 +12,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -282,6 +284,25 @@ struct lpk_clock {
     }
 };
 
+int64_t lpk_clock_flicker_len(double duration_s) {
+    if (!(duration_s >= 0.0) || !std::isfinite(duration_s) || duration_s > 1e9) return -1;
+    return (int64_t)std::ceil(duration_s * kFlickerRate) + 2;
+}
+
+lpk_status lpk_clock_flicker_table(const lpk_clock_cfg *spec, uint64_t seed, double *out, int64_t n) {
+    if (!spec || !out || n < 0) return lpk::fail(nullptr, LPK_EINVAL, "NULL spec or output, or n < 0");
+    if (!(spec->flicker_floor > 0.0) || !std::isfinite(spec->flicker_floor))
+        return lpk::fail(nullptr, LPK_EINVAL, "the clock has no flicker floor");
+    // the host stream's flicker, advanced point by point: D[m] after the
+    // step that moves its frontier to m (Flicker::advance_to, clock/mod.rs:130-140)
+    Flicker f(spec->flicker_floor, Xoshiro(seed));
+    for (int64_t m = 0; m < n; ++m) {
+        f.hi += f.step(f.state, f.rng) * f.scale / kFlickerRate;
+        out[m] = f.hi;
+    }
+    return LPK_OK;
+}
+
 namespace {
 
 struct TxHost {
@@ -311,6 +332,11 @@ struct lpk_scene {
     std::vector<TxHost> tx;
     std::vector<RxHost> rx;
     std::vector<std::pair<int32_t, int32_t>> work;
+    // flicker tracks handed out by lpk_scene_band_desc, per (receiver, clock
+    // seed); entries are never erased, so a descriptor's pointer stays valid
+    // while the scene lives
+    std::mutex flicker_mu;
+    std::map<std::pair<int32_t, uint64_t>, std::vector<double>> flicker;
 };
 
 namespace {
@@ -663,8 +689,35 @@ lpk_status lpk_scene_band_desc(const lpk_scene *s, int32_t r, int32_t b, uint64_
         if (fe.has_adc) d->post[d->n_post++] = {LPK_POST_ADC, fe.adc_bits, fe.adc_full_scale_v};
     }
     d->solver = LPK_SOLVER_REFERENCE;
+    if (rx.clock.flicker_floor > 0.0) {  // the scene's flicker track of this receiver clock
+        lpk_scene *ms = const_cast<lpk_scene *>(s);
+        std::lock_guard<std::mutex> lk(ms->flicker_mu);
+        std::vector<double> &tab = ms->flicker[{r, d->clock_seed}];
+        if (tab.empty()) {
+            const int64_t len = lpk_clock_flicker_len(s->cfg.duration_s);
+            if (len < 2) return host_fail(LPK_EINVAL, "scene duration out of range for the flicker track");
+            tab.resize((size_t)len);
+            lpk_status st = lpk_clock_flicker_table(&rx.clock, d->clock_seed, tab.data(), len);
+            if (st) {
+                tab.clear();
+                return st;
+            }
+        }
+        d->flicker_delta_s = tab.data();
+        d->flicker_n = (int64_t)tab.size();
+    }
     return LPK_OK;
 }
+
+namespace {
+// A device clock for a band whose descriptor has a random (host-stream)
+// clock: the white-FM walk on the device when the clock has one, the flicker
+// track (if any) through the descriptor, the deterministic part otherwise.
+void use_device_clock(lpk_band_desc &d, const lpk_clock_cfg &clk) {
+    if (d.clock_mode != LPK_CLOCK_HOST) return;
+    d.clock_mode = clk.allan_deviation_1s > 0.0 ? LPK_CLOCK_DEVICE_WALK : LPK_CLOCK_DETERMINISTIC;
+}
+}  // namespace
 
 lpk_status lpk_generate_band(lpk_scene *s, int32_t r, int32_t b, uint64_t seed_base, int32_t work_idx,
                              int64_t chunk_samples, int32_t flags, lpk_sink_fn sink, void *user,
@@ -677,11 +730,9 @@ lpk_status lpk_generate_band(lpk_scene *s, int32_t r, int32_t b, uint64_t seed_b
     if (!(flags & LPK_NOISE_ON)) d.noise_power_w = 0.0;
     if (flags & LPK_GEN_SPLIT) d.solver = LPK_SOLVER_SPLIT;
     const RxHost &rx = s->rx[r];
-    // The device walk covers the white-FM part; flicker and moving receivers
-    // (whose positions need Δt on the host) keep the host stream.
-    if ((flags & LPK_GEN_DEVICE_CLOCK) && d.clock_mode == LPK_CLOCK_HOST && rx.stationary &&
-        !(rx.clock.flicker_floor > 0.0))
-        d.clock_mode = LPK_CLOCK_DEVICE_WALK;
+    // The device clock covers the white-FM walk and the flicker track; moving
+    // receivers (whose positions need Δt on the host) keep the host stream.
+    if ((flags & LPK_GEN_DEVICE_CLOCK) && rx.stationary) use_device_clock(d, rx.clock);
     const int64_t n = lpk_scene_band_samples(s, r, b);
     if (chunk_samples < 1) chunk_samples = 1;
     std::vector<int32_t> active(256);
@@ -765,9 +816,7 @@ lpk_status lpk_generate_scene(lpk_scene *s, uint64_t seed_base, double round_s, 
         if (!(flags & LPK_NOISE_ON)) u.band.noise_power_w = 0.0;
         if (flags & LPK_GEN_SPLIT) u.band.solver = LPK_SOLVER_SPLIT;
         const RxHost &rx = s->rx[r];
-        if ((flags & LPK_GEN_DEVICE_CLOCK) && u.band.clock_mode == LPK_CLOCK_HOST && rx.stationary &&
-            !(rx.clock.flicker_floor > 0.0))
-            u.band.clock_mode = LPK_CLOCK_DEVICE_WALK;
+        if ((flags & LPK_GEN_DEVICE_CLOCK) && rx.stationary) use_device_clock(u.band, rx.clock);
         if (!rx.stationary || u.band.clock_mode == LPK_CLOCK_HOST) {
             rest.push_back(w);
             continue;

@@ -129,6 +129,16 @@ cudaError_t launch_walk_materialize(uint64_t seed, double sigma, const double *d
 lpk_status prepare_walk(lpk_ctx *ctx, const lpk_band_desc *d, int64_t i0, int64_t n, DevBand &b, double *d_eps,
                         int64_t eps_cap);
 int64_t walk_span(const lpk_band_desc *d, int64_t i0, int64_t n, int64_t *kA);
+// Device-clock inputs of a band chunk in one scratch region: the walk
+// values (DEVICE_WALK) followed by the staged flicker points (a flicker
+// track). clock_region_bytes: the region's size (256-byte aligned parts);
+// prepare_clock fills it and points b at it (lpk_abi.cu).
+size_t clock_region_bytes(const lpk_band_desc *d, int64_t i0, int64_t n);
+lpk_status prepare_clock(lpk_ctx *ctx, const lpk_band_desc *d, int64_t i0, int64_t n, DevBand &b, char *region);
+// The flicker points of a chunk copied to dst (at most cap) and b pointed
+// at them; nothing without a flicker track.
+lpk_status stage_flicker(lpk_ctx *ctx, const lpk_band_desc *d, int64_t i0, int64_t n, DevBand &b, double *dst,
+                         int64_t cap);
 // Record a profiling event pair around a fan-out launch (no-op when off).
 void prof_begin(lpk_ctx *ctx);
 void prof_end(lpk_ctx *ctx);

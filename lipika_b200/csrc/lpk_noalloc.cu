@@ -7,7 +7,8 @@
 // lpk_band_chunk_device_static does what lpk_band_chunk_device does — the
 // active list, the per-transmitter occlusion words, the receiver clock walk
 // (block totals, group sums, carries, the materialised walk) and, for a
-// split-solver band, the anchor records of the chunk's tiles — in one
+// split-solver band, the anchor records of the chunk's tiles, and the
+// flicker points of a clock with a flicker track — in one
 // file-scope static device array instead of the context's growable scratch,
 // running the same kernels on the same inputs (so the outputs are the same
 // bits).
@@ -38,7 +39,9 @@ constexpr size_t kOffGsum = kOffCarry + sizeof(double) * (kMaxWalkBlocks + 1);
 constexpr size_t kOffEps = (kOffGsum + sizeof(double) * (kMaxWalkBlocks / lpk::kGroupBlocks + 1) + 255) / 256 * 256;
 constexpr size_t kOffRecs = (kOffEps + sizeof(double) * kMaxWalkSpan + 255) / 256 * 256;
 constexpr size_t kMaxRecsBytes = size_t(12) << 20;  // split anchor records: 32,768 (tile, transmitter) pairs
-constexpr size_t kStaticBytes = kOffRecs + kMaxRecsBytes;  // 22.0 MiB
+constexpr size_t kOffFlicker = kOffRecs + kMaxRecsBytes;
+constexpr int64_t kMaxFlicker = 8192;             // flicker track points one chunk may read (64 s)
+constexpr size_t kStaticBytes = kOffFlicker + sizeof(double) * kMaxFlicker;  // 22.1 MiB
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
 
@@ -114,6 +117,8 @@ extern "C" lpk_status lpk_band_chunk_device_static(lpk_ctx *c, const lpk_band_de
         b.eps_k0 = kA;
         b.fm = band->clock_master_rate_hz;
     }
+    if (e == cudaSuccess && (st = stage_flicker(c, band, i0, n, b, (double *)(base + kOffFlicker), kMaxFlicker)))
+        return st;
     if (e == cudaSuccess && split) {  // the split path of lpk_band_chunk_device, on one stream
         b.unocc_words = b.has_antenna ? d_words : nullptr;
         e = launch_band_split(c->split_variant, b, c->d_tx, d_active, n_active, base + kOffRecs, (float2 *)d_out,

@@ -84,6 +84,7 @@ class BandDesc(C.Structure):
         ("ant_fb_db", C.c_double), ("ant_cutoff_deg", C.c_double),
         ("n_post", C.c_int32), ("solver", C.c_int32),
         ("post", PostOp * 3),
+        ("flicker_delta_s", C.POINTER(C.c_double)), ("flicker_n", C.c_int64),
     ]
 
 
@@ -190,6 +191,8 @@ SIGNATURES = {
                                 C.c_double, C.c_double, C.c_int64, C.c_int32, C.c_int32, C.c_float, C.c_uint64, _F]),
     "lpk_clock_new": (C.c_int32, [C.POINTER(A.ClockCfg), C.c_double, C.c_double, C.c_uint64, C.POINTER(_VP)]),
     "lpk_clock_delta_t": (C.c_int32, [_VP, _D, C.c_int64, _D]),
+    "lpk_clock_flicker_len": (C.c_int64, [C.c_double]),
+    "lpk_clock_flicker_table": (C.c_int32, [C.POINTER(A.ClockCfg), C.c_uint64, _D, C.c_int64]),
     "lpk_clock_free": (None, [_VP]),
 }
 

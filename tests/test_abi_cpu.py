@@ -133,6 +133,51 @@ def test_host_clock_stream_matches_oracle_bit_for_bit():
     assert got.tobytes() == exp.tobytes()
 
 
+def test_flicker_track_is_the_oracle_stream_flicker():
+    """lpk_clock_flicker_table (the device clocks' flicker input) holds the
+    oracle stream's flicker at the coarse points, and its linear
+    interpolation (Flicker::delta_at, src/clock/mod.rs:142-148) reproduces the
+    stream at every sample time, bit for bit."""
+    spec = A.ClockCfg(0.0, 3e-10, 0.0, 0.0)
+    L = N.lib()
+    n = L.lpk_clock_flicker_len(5.0)
+    assert n == 5 * 128 + 2
+    tab = np.zeros(n)
+    N.check(L.lpk_clock_flicker_table(C.byref(spec), 31, N.dptr(tab), n))
+    oc = O.lib().orc_clock_new(C.byref(spec), 0.0, 48_000.0, 31)
+    t = np.arange(0, 5 * 48_000, 7, dtype=np.float64) / 48_000.0
+    exp = np.array([O.lib().orc_clock_delta_t_at(oc, x) for x in t])
+    O.lib().orc_clock_free(oc)
+    x = t * 128.0
+    fl = np.floor(x)
+    m = fl.astype(np.int64)
+    frac = x - fl
+    got = 0.0 + (tab[m] * (1.0 - frac) + tab[m + 1] * frac)  # (ε = 0 + flicker) + (c + m t = 0)
+    assert got.tobytes() == (exp + 0.0).tobytes()
+    assert np.std(np.diff(tab)) > 0.0
+    bad = A.ClockCfg(1e-11, 0.0, 0.0, 0.0)
+    assert L.lpk_clock_flicker_table(C.byref(bad), 31, N.dptr(tab), n) == N.LPK_EINVAL
+
+
+def test_band_desc_carries_the_scene_flicker_track():
+    sc = scenes.config_c0(duration_s=2.0, clock=cfg.Clock(allan_deviation_1s=1e-11, flicker_floor=2e-10))
+    hs = HostScene(sc)
+
+    def desc():
+        d = N.BandDesc()
+        N.check(N.lib().lpk_scene_band_desc(hs.h, 0, 0, 2026, 0, C.byref(d)))
+        return d
+    d = desc()
+    assert d.flicker_n == 2 * 128 + 2 and bool(d.flicker_delta_s)
+    tab = np.ctypeslib.as_array(d.flicker_delta_s, (d.flicker_n,)).copy()
+    exp = np.zeros(d.flicker_n)
+    spec = A.ClockCfg(1e-11, 2e-10, sc.receivers[0].clock.frequency_offset_y0,
+                      sc.receivers[0].clock.initial_time_offset_s)
+    N.check(N.lib().lpk_clock_flicker_table(C.byref(spec), d.clock_seed, N.dptr(exp), d.flicker_n))
+    assert tab.tobytes() == exp.tobytes()
+    assert C.addressof(desc().flicker_delta_s.contents) == C.addressof(d.flicker_delta_s.contents)  # one track
+
+
 def test_host_clock_with_flicker_matches_oracle():
     spec = A.ClockCfg(0.0, 1e-10, 0.0, 0.0)
     L = N.lib()

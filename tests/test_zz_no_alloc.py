@@ -4,8 +4,8 @@ A host that renders from a real-time thread, or one that owns the whole
 device through its own pool, cannot let the library call cudaMalloc while it
 renders. The static entry point keeps its working memory in one file-scope
 device array instead; these checks call it through the C ABI and compare it
-with lpk_band_chunk_device, chunk after chunk, for both solvers and with an
-antenna (the array keeps the previous call's contents, so the second call
+with lpk_band_chunk_device, chunk after chunk, for both solvers, with a
+flicker clock and with an antenna (the array keeps the previous call's contents, so the second call
 shows nothing stale leaks through), and time the walk rebuild it does on
 every call.
 This file is collected last on purpose.
@@ -66,6 +66,23 @@ def test_static_scratch_matches_allocating_entry_point_two_calls():
         d.solver = solver
         # two calls in a row, the second earlier in the band
         _compare_two_calls(ctx, prep, d, r, b, 500_000, (3_000_000, 123_457), lambda k: [1] * k)
+    prep.close()
+    ctx.close()
+
+
+def test_static_scratch_flicker_clock_both_solvers():
+    """A receiver clock with a white-FM walk and a flicker floor: the static
+    entry point stages the chunk's flicker points in its array too."""
+    from lipika_b200 import config as cfg
+    ctx = N.Context(0)
+    clock = cfg.Clock(allan_deviation_1s=1e-11, flicker_floor=3e-10, frequency_offset_y0=0.4e-6)
+    prep = P.Prepared(scenes.config_c1(duration_s=3.0, clock=clock), ctx)
+    d = prep.band_desc(0, 1, 2026, 1)
+    d.clock_mode = N.LPK_CLOCK_DEVICE_WALK
+    assert d.flicker_n > 0
+    for solver in (N.LPK_SOLVER_REFERENCE, N.LPK_SOLVER_SPLIT):
+        d.solver = solver
+        _compare_two_calls(ctx, prep, d, 0, 1, 400_000, (2_000_000, 77_777), lambda k: [1] * k)
     prep.close()
     ctx.close()
 
