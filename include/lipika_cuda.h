@@ -152,7 +152,11 @@ lpk_status lpk_kepler_tables(lpk_ctx *ctx, const lpk_kepler_orbit *orbits, int32
                              double dt_s, int64_t n_points, double *grid_xyz);
 
 enum { LPK_CLOCK_HOST = 0, LPK_CLOCK_DETERMINISTIC = 1, LPK_CLOCK_DEVICE_WALK = 2 };
-enum { LPK_RX_STATIONARY = 0, LPK_RX_PER_SAMPLE = 1 };
+/* LPK_RX_KEPLER: a receiver on a circular Keplerian orbit (lpk_band_desc
+ * rx_orbit), positioned on the device at each sample's rounded absolute UTC
+ * time exactly as receiver.trajectory.position_ecef_batch(epoch + t_utc)
+ * does (src/pipeline.rs:929-931, src/geometry/kepler.rs:32-85). */
+enum { LPK_RX_STATIONARY = 0, LPK_RX_PER_SAMPLE = 1, LPK_RX_KEPLER = 2 };
 enum { LPK_POST_GAIN = 0, LPK_POST_NONLINEARITY = 1, LPK_POST_ADC = 2 };
 /* Fan-out solvers: REFERENCE, the reference's per-sample f64 arithmetic in
  * its order (bit-exact emission times, indices and ADC codes); SPLIT, the
@@ -206,6 +210,7 @@ typedef struct lpk_band_desc {
      * scene owns that table. */
     const double *flicker_delta_s;
     int64_t flicker_n;
+    lpk_kepler_orbit rx_orbit;  /* LPK_RX_KEPLER: the receiver's orbit */
 } lpk_band_desc;
 
 /* One chunk of one band through the fan-out, Σ, AWGN and rx chain.

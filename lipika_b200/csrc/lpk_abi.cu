@@ -87,8 +87,18 @@ lpk_status build_dev_band(lpk_ctx *ctx, const lpk_band_desc *d, int64_t i0, int6
     if (!(d->noise_power_w >= 0.0) && !(d->noise_power_w < 0.0))
         return fail(ctx, LPK_EINVAL, "band noise_power_w is NaN");
     if (n < 0 || i0 < 0) return fail(ctx, LPK_EINVAL, "chunk start and length must be non-negative");
-    if (d->rx_kind != LPK_RX_STATIONARY && d->rx_kind != LPK_RX_PER_SAMPLE)
+    if (d->rx_kind != LPK_RX_STATIONARY && d->rx_kind != LPK_RX_PER_SAMPLE && d->rx_kind != LPK_RX_KEPLER)
         return fail(ctx, LPK_EINVAL, "unknown rx_kind");
+    if (d->rx_kind == LPK_RX_KEPLER) {
+        if (!make_orbit(d->rx_orbit, b.rx_orb)) return fail(ctx, LPK_EINVAL, "bad receiver orbit");
+        // fl(epoch + tu) - orbit epoch is exact (Sterbenz) when the orbit
+        // epoch is 0 or within a factor of two of every query time; then the
+        // split path's smooth receiver model plus the query's rounding offset
+        // is the reference's orbit time
+        const double e0 = d->rx_orbit.epoch_unix, ep = d->epoch_unix;
+        b.rx_de = ep - e0;
+        b.rx_split_ok = e0 == 0.0 || (ep > 0.0 && e0 >= 0.6 * ep && e0 <= 1.6 * ep);
+    }
     if (d->clock_mode != LPK_CLOCK_HOST && d->clock_mode != LPK_CLOCK_DETERMINISTIC &&
         d->clock_mode != LPK_CLOCK_DEVICE_WALK)
         return fail(ctx, LPK_EINVAL, "unknown clock_mode");
@@ -709,8 +719,8 @@ lpk_status lpk_split_accuracy(lpk_ctx *c, const lpk_band_desc *band, const int32
                               int64_t i0, int64_t n, const double *d_delta, lpk_cf32 *d_out, double *max_delay_err_s,
                               double *max_phase_err_rad, int64_t *n_fast, int64_t *n_exact) {
     if (!c) return fail(nullptr, LPK_EINVAL, "ctx is NULL");
-    if (!band || band->solver != LPK_SOLVER_SPLIT || band->rx_kind != LPK_RX_STATIONARY)
-        return fail(c, LPK_EINVAL, "accuracy mode needs a split-solver band with a stationary receiver");
+    if (!band || !use_split(band))
+        return fail(c, LPK_EINVAL, "accuracy mode needs a split-solver band with a stationary or orbiting receiver");
     if (!max_delay_err_s || !max_phase_err_rad || !n_fast || !n_exact)
         return fail(c, LPK_EINVAL, "accuracy outputs are NULL");
     DevBand b;

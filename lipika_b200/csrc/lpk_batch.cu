@@ -145,6 +145,8 @@ k_batch_carry(const DevWalk *__restrict__ walks, const RoundDesc *__restrict__ r
 // Anchor fits of every (slot, tile, transmitter) of the round, one per
 // thread; each block builds its run of records in shared memory and stores
 // it contiguously.
+// MOV: some unit's receiver is on an orbit (compiled apart, as the fan-out).
+template <bool MOV>
 __global__ void __launch_bounds__(kAnchorThreads, LPK_ANCHOR_MINB)
 k_batch_anchor(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ units,
                const DevTx *__restrict__ txs, const int32_t *__restrict__ act, const RoundDesc *__restrict__ rd,
@@ -163,8 +165,13 @@ k_batch_anchor(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ 
             const int64_t tile = local / bu.n_active;
             const int k = (int)(local - tile * bu.n_active);
             const int64_t gs = (ru.t0 + tile) * tile_len;
-            fit_anchor(bands[ru.unit], txs[act[bu.act_off + k]], gs, gs + tile_len - 1, bu.exact_only != 0,
-                       srec[threadIdx.x], exts + id);
+            const DevBand &band = bands[ru.unit];
+            if (MOV && band.rx_kind == LPK_RX_KEPLER)
+                fit_anchor<true>(band, txs[act[bu.act_off + k]], gs, gs + tile_len - 1, bu.exact_only != 0,
+                                 srec[threadIdx.x], exts + id);
+            else
+                fit_anchor<false>(band, txs[act[bu.act_off + k]], gs, gs + tile_len - 1, bu.exact_only != 0,
+                                  srec[threadIdx.x], exts + id);
         }
         __syncthreads();
         store_recs(srec, recs + base, (int)(total - base < kAnchorThreads ? total - base : kAnchorThreads));
@@ -177,7 +184,10 @@ k_batch_anchor(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ 
 // (the claim's latency is hidden and the end-of-tile barrier publishes it).
 // A block restages the band and its transmitters only when the next tile
 // belongs to another unit.
-template <int TILE, int THREADS, int MINB>
+// MOV: some unit's receiver is on an orbit; its tiles take the orbit-aware
+// tile code (compiled apart, so batches of stationary receivers run kernels
+// without it).
+template <int TILE, int THREADS, int MINB, bool MOV>
 __global__ void __launch_bounds__(THREADS, MINB)
 k_batch_fanout(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ units,
                const DevTx *__restrict__ txs, const int32_t *__restrict__ act, const DevWalk *__restrict__ walks,
@@ -217,9 +227,15 @@ k_batch_fanout(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ 
         cur = ru.unit;
         __syncthreads();
         const int64_t first = (ru.t0 + local) * TILE - ru.i0;
-        split_tile<TILE / THREADS, THREADS, false, false>(*sb, stx, srec, exts + ru.rec_off + local * bu.n_active,
-                                                          bu.n_active, first, bu.out[rd->parity], nullptr, nullptr,
-                                                   nullptr);
+        const AnchorExt *xrec = exts + ru.rec_off + local * bu.n_active;
+        if (MOV && sb->rx_kind == LPK_RX_KEPLER)  // block-uniform
+            split_tile<TILE / THREADS, THREADS, false, false, false, true>(*sb, stx, srec, xrec, bu.n_active, first,
+                                                                           bu.out[rd->parity], nullptr, nullptr,
+                                                                           nullptr);
+        else
+            split_tile<TILE / THREADS, THREADS, false, false, false, false>(*sb, stx, srec, xrec, bu.n_active, first,
+                                                                            bu.out[rd->parity], nullptr, nullptr,
+                                                                            nullptr);
         __syncthreads();  // the next stage overwrites the shared tiles
     }
 }
@@ -230,9 +246,9 @@ using FanoutKernel = void (*)(const DevBand *, const BatchUnit *, const DevTx *,
 
 struct FanoutShape {
     int tile, threads;
-    FanoutKernel kern;
+    FanoutKernel kern[2];  // [some receiver on an orbit]
 };
-#define LPK_BATCH_ENTRY(I, T, N, M) {T, N, k_batch_fanout<T, N, M>},
+#define LPK_BATCH_ENTRY(I, T, N, M) {T, N, {k_batch_fanout<T, N, M, false>, k_batch_fanout<T, N, M, true>}},
 const FanoutShape kFanout[kSplitVariants] = {LPK_SPLIT_VARIANTS(LPK_BATCH_ENTRY)};
 #undef LPK_BATCH_ENTRY
 
@@ -284,6 +300,7 @@ struct lpk_batch {
     int64_t recs_cap = 0;
     int64_t n_rounds = 0;
     int32_t max_active = 0;
+    int any_orbit = 0;                              // some unit's receiver is on an orbit
     int variant = 0, bps = 0, max_bps = 0, walk_grid = 0, anchor_grid = 0;
     cudaGraph_t graph_src[2] = {nullptr, nullptr};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -403,7 +420,8 @@ lpk_status build_graph(lpk_batch *b, int p) {
     lpk_ctx *c = b->ctx;
     const FanoutShape &sh = kFanout[b->variant];
     const size_t smem = fanout_smem(b->max_active);
-    cudaError_t e = cudaFuncSetAttribute(sh.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const FanoutKernel kern = sh.kern[b->any_orbit];
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_fail(c, e, "batch fan-out shared memory");
     int dev_sms = 0;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
@@ -414,7 +432,7 @@ lpk_status build_graph(lpk_batch *b, int p) {
     cudaMemcpyAsync(b->d_round, b->h_round[p], sizeof(RoundDesc), cudaMemcpyHostToDevice, c->stream);
     cudaEventRecord(b->fork, c->stream);
     cudaStreamWaitEvent(b->side, b->fork, 0);
-    k_batch_anchor<<<b->anchor_grid, kAnchorThreads, 0, b->side>>>(b->d_bands, b->d_units, c->d_tx, b->d_act, b->d_round,
+    (b->any_orbit ? k_batch_anchor<true> : k_batch_anchor<false>)<<<b->anchor_grid, kAnchorThreads, 0, b->side>>>(b->d_bands, b->d_units, c->d_tx, b->d_act, b->d_round,
                                                         b->d_recs, b->d_exts);
     cudaEventRecord(b->join, b->side);
     if (!b->walks.empty()) {
@@ -425,7 +443,7 @@ lpk_status build_graph(lpk_batch *b, int p) {
     cudaStreamWaitEvent(c->stream, b->join, 0);
     cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned long long), c->stream);
     if (prof) cudaEventRecordWithFlags(b->mark[0], c->stream, cudaEventRecordExternal);
-    sh.kern<<<(unsigned)(dev_sms * b->bps), sh.threads, smem, c->stream>>>(
+    kern<<<(unsigned)(dev_sms * b->bps), sh.threads, smem, c->stream>>>(
         b->d_bands, b->d_units, c->d_tx, b->d_act, b->d_walks, b->d_round, b->d_recs, b->d_exts, b->d_counter,
         b->max_active);
     if (prof) cudaEventRecordWithFlags(b->mark[1], c->stream, cudaEventRecordExternal);
@@ -469,10 +487,11 @@ lpk_status configure(lpk_batch *b, int variant, int bps) {
     if (variant < 0 || variant >= kSplitVariants) return fail(b->ctx, LPK_EINVAL, "unknown split variant");
     const FanoutShape &sh = kFanout[variant];
     const size_t smem = fanout_smem(b->max_active);
-    cudaError_t e = cudaFuncSetAttribute(sh.kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const FanoutKernel kern = sh.kern[b->any_orbit];
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_fail(b->ctx, e, "batch fan-out shared memory");
     int occ = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sh.kern, sh.threads, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, sh.threads, smem);
     if (e != cudaSuccess) return cuda_fail(b->ctx, e, "batch occupancy query");
     if (occ < 1) return fail(b->ctx, LPK_EINVAL, "batch fan-out does not fit on an SM");
     if (bps < 0) return fail(b->ctx, LPK_EINVAL, "blocks per SM must be >= 0");
@@ -568,8 +587,8 @@ lpk_status lpk_batch_create(lpk_ctx *c, const lpk_work_unit *wu, int32_t n_units
         uh.n_samples = w.n_samples;
         uh.n_active = w.n_active;
         if (w.n_samples < 0) st = fail(c, LPK_EINVAL, "work unit length must be >= 0");
-        else if (w.band.rx_kind != LPK_RX_STATIONARY)
-            st = fail(c, LPK_ENOTSUP, "batch units need a stationary receiver");
+        else if (w.band.rx_kind != LPK_RX_STATIONARY && w.band.rx_kind != LPK_RX_KEPLER)
+            st = fail(c, LPK_ENOTSUP, "batch units need a stationary or orbiting receiver (not per-sample positions)");
         else if (w.band.clock_mode != LPK_CLOCK_DETERMINISTIC && w.band.clock_mode != LPK_CLOCK_DEVICE_WALK)
             st = fail(c, LPK_ENOTSUP, "batch units need a deterministic or device-walk clock");
         else if ((st = build_dev_band(c, &w.band, 0, w.n_samples, h_bands[u]))) {
@@ -603,6 +622,7 @@ lpk_status lpk_batch_create(lpk_ctx *c, const lpk_work_unit *wu, int32_t n_units
         bu.exact_only = uh.exact_only;
         for (int k = 0; k < w.n_active; ++k) h_act.push_back(w.active[k]);
         b->max_active = std::max(b->max_active, w.n_active);
+        if (w.band.rx_kind == LPK_RX_KEPLER) b->any_orbit = 1;
         b->units.push_back(uh);
         b->h_units.push_back(bu);
     }

@@ -48,8 +48,17 @@ __device__ __forceinline__ double band_delta(const DevBand &b, int64_t j, double
     return b.delta[j];
 }
 
-__device__ __forceinline__ void band_rx(const DevBand &b, int64_t j, double &ox, double &oy, double &oz) {
+// Receiver position of chunk sample j at epoch-relative UTC time tu:
+// receiver.trajectory.position_ecef_batch(epoch + t_utc) (src/pipeline.rs:
+// 929-931) — a constant, the orbit at the rounded absolute time, or the
+// caller's per-sample positions.
+__device__ __forceinline__ void band_rx(const DevBand &b, int64_t j, double tu, double &ox, double &oy,
+                                        double &oz) {
     if (b.rx_kind == LPK_RX_STATIONARY) { ox = b.rx[0]; oy = b.rx[1]; oz = b.rx[2]; return; }
+    if (b.rx_kind == LPK_RX_KEPLER) {
+        kepler_at(b.rx_orb, __dsub_rn(__dadd_rn(b.epoch, tu), b.rx_orb.epoch), ox, oy, oz);
+        return;
+    }
     ox = b.rxpos[j];
     oy = b.rxpos[b.n + j];
     oz = b.rxpos[2 * b.n + j];

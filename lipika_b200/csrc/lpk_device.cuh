@@ -56,6 +56,43 @@ struct __align__(16) DevTx {
 };
 static_assert(sizeof(DevTx) % 16 == 0, "DevTx arrays must keep 16-byte alignment");
 
+// A circular Keplerian orbit (CircularKeplerian, src/geometry/kepler.rs:32-85)
+// with its per-orbit constants computed once on the host: radius, mean
+// motion, true anomaly at epoch (rad), sines and cosines of inclination and
+// RAAN, epoch (unix s).
+struct DevOrbit {
+    double r, mm, nu0, si, ci, so, co, epoch;
+};
+
+// CircularKeplerian::position_ecef at orbit time e = t - epoch, in the
+// host's operation order (explicit rounding); with vel, also the ECEF
+// velocity, the exact time derivative of that expression (ν' = mean motion,
+// θ' = ω⊕).
+__device__ __forceinline__ void kepler_at(const DevOrbit &k, double e, double &x, double &y, double &z,
+                                          double *vel = nullptr) {
+    const double nu = __dadd_rn(k.nu0, __dmul_rn(k.mm, e));
+    double snu, cnu;
+    sincos(nu, &snu, &cnu);
+    const double xp = __dmul_rn(k.r, cnu), yp = __dmul_rn(k.r, snu);
+    const double y1 = __dmul_rn(yp, k.ci), z1 = __dmul_rn(yp, k.si);
+    const double xe = __dsub_rn(__dmul_rn(xp, k.co), __dmul_rn(y1, k.so));
+    const double ye = __dadd_rn(__dmul_rn(xp, k.so), __dmul_rn(y1, k.co));
+    const double th = __dmul_rn(kEarthRate, e);
+    double s, c;
+    sincos(th, &s, &c);
+    x = __dadd_rn(__dmul_rn(xe, c), __dmul_rn(ye, s));
+    y = __dadd_rn(__dmul_rn(-xe, s), __dmul_rn(ye, c));
+    z = z1;
+    if (vel) {
+        const double xpd = -yp * k.mm, ypd = xp * k.mm;
+        const double y1d = ypd * k.ci;
+        const double xed = xpd * k.co - y1d * k.so, yed = xpd * k.so + y1d * k.co;
+        vel[0] = xed * c + yed * s + y * kEarthRate;
+        vel[1] = -xed * s + yed * c - x * kEarthRate;
+        vel[2] = ypd * k.si;
+    }
+}
+
 // Per-band constants (host-computed where the reference computes them once).
 struct DevBand {
     double epoch, fs, lo, inv_c;
@@ -86,6 +123,12 @@ struct DevBand {
                                         // error) as double bits, (fast-path, exact-path) sample counts
     int32_t post_kind[3];
     float post_a[3], post_b[3];         // gain: g | nonlin: k | adc: fs, lsb
+    DevOrbit rx_orb;                    // rx kind KEPLER: the receiver's orbit
+    double rx_de;                       // KEPLER: epoch - rx_orb.epoch (exact), so the orbit time of
+                                        // epoch-relative UTC tu is rx_de + tu without rounding epoch + tu
+    int32_t rx_split_ok;                // KEPLER: fl(fl(epoch + tu) - orbit epoch) is exact for every tu of
+                                        // the scene, so the split path's smooth receiver model holds
+    int32_t rx_reserved;
 };
 
 // ---------------------------------------------------------------- helpers

@@ -662,8 +662,16 @@ lpk_status lpk_scene_band_desc(const lpk_scene *s, int32_t r, int32_t b, uint64_
     d->noise_power_w = band.has_noise_power ? band.noise_power_w
                                             : kBoltzmann * band.noise_temperature_k * band.sample_rate_hz;
     d->noise_seed = seed_base + (uint64_t)work_idx;  // noise_seed, pipeline.rs:828-830
-    d->rx_kind = rx.stationary ? LPK_RX_STATIONARY : LPK_RX_PER_SAMPLE;
     for (int k = 0; k < 3; ++k) d->rx_ecef[k] = rx.pos[k];
+    if (rx.stationary) {
+        d->rx_kind = LPK_RX_STATIONARY;
+    } else if (rx.traj.kind == LPK_TRAJ_CIRCULAR_KEPLERIAN) {  // positioned on the device per sample
+        d->rx_kind = LPK_RX_KEPLER;
+        d->rx_orbit = {rx.traj.semi_major_axis_m, rx.traj.inclination_deg, rx.traj.raan_deg,
+                       rx.traj.true_anomaly_deg_at_epoch, rx.traj.epoch_unix};
+    } else {
+        d->rx_kind = LPK_RX_PER_SAMPLE;
+    }
     bool random_clock = rx.clock.allan_deviation_1s > 0.0 || rx.clock.flicker_floor > 0.0;
     d->clock_mode = random_clock ? LPK_CLOCK_HOST : LPK_CLOCK_DETERMINISTIC;
     d->clock_offset_s = rx.clock.initial_time_offset_s;
@@ -730,9 +738,9 @@ lpk_status lpk_generate_band(lpk_scene *s, int32_t r, int32_t b, uint64_t seed_b
     if (!(flags & LPK_NOISE_ON)) d.noise_power_w = 0.0;
     if (flags & LPK_GEN_SPLIT) d.solver = LPK_SOLVER_SPLIT;
     const RxHost &rx = s->rx[r];
-    // The device clock covers the white-FM walk and the flicker track; moving
-    // receivers (whose positions need Δt on the host) keep the host stream.
-    if ((flags & LPK_GEN_DEVICE_CLOCK) && rx.stationary) use_device_clock(d, rx.clock);
+    // The device clock covers the white-FM walk and the flicker track; a
+    // receiver whose positions the host computes keeps the host stream.
+    if ((flags & LPK_GEN_DEVICE_CLOCK) && d.rx_kind != LPK_RX_PER_SAMPLE) use_device_clock(d, rx.clock);
     const int64_t n = lpk_scene_band_samples(s, r, b);
     if (chunk_samples < 1) chunk_samples = 1;
     std::vector<int32_t> active(256);
@@ -749,7 +757,8 @@ lpk_status lpk_generate_band(lpk_scene *s, int32_t r, int32_t b, uint64_t seed_b
     std::vector<double> t_local, delta, rxpos;
     std::vector<lpk_cf32> out((size_t)cap);
     if (clock) { t_local.resize((size_t)cap); delta.resize((size_t)cap); }
-    if (!rx.stationary) rxpos.resize(3 * (size_t)cap);
+    const bool host_rx = d.rx_kind == LPK_RX_PER_SAMPLE;
+    if (host_rx) rxpos.resize(3 * (size_t)cap);
     const double fs = d.fs_hz, epoch = d.epoch_unix;
     int64_t i0 = 0;
     while (i0 < n) {
@@ -759,7 +768,7 @@ lpk_status lpk_generate_band(lpk_scene *s, int32_t r, int32_t b, uint64_t seed_b
             for (int64_t j = 0; j < clen; ++j) t_local[j] = (double)(i0 + j) / fs;  // pipeline.rs:918
             for (int64_t j = 0; j < clen; ++j) delta[j] = clock->delta_t_at(t_local[j]);
         }
-        if (!rx.stationary) {  // receiver.position_ecef_batch(epoch + t_utc), pipeline.rs:929-931
+        if (host_rx) {  // receiver.position_ecef_batch(epoch + t_utc), pipeline.rs:929-931
             for (int64_t j = 0; j < clen; ++j) {
                 double tl = (double)(i0 + j) / fs;
                 double dl = clock ? delta[j] : d.clock_offset_s + d.clock_y0 * tl;
@@ -771,7 +780,7 @@ lpk_status lpk_generate_band(lpk_scene *s, int32_t r, int32_t b, uint64_t seed_b
             }
         }
         st = lpk_band_chunk(s->ctx, &d, active.data(), na, i0, clen, clock ? delta.data() : nullptr,
-                            rx.stationary ? nullptr : rxpos.data(), out.data(), res->unoccluded);
+                            host_rx ? rxpos.data() : nullptr, out.data(), res->unoccluded);
         if (st) return st;
         int32_t flow = sink(user, out.data(), clen);
         if (flow < 0) return host_fail(LPK_EINVAL, "sink reported an error");
@@ -816,8 +825,8 @@ lpk_status lpk_generate_scene(lpk_scene *s, uint64_t seed_base, double round_s, 
         if (!(flags & LPK_NOISE_ON)) u.band.noise_power_w = 0.0;
         if (flags & LPK_GEN_SPLIT) u.band.solver = LPK_SOLVER_SPLIT;
         const RxHost &rx = s->rx[r];
-        if ((flags & LPK_GEN_DEVICE_CLOCK) && rx.stationary) use_device_clock(u.band, rx.clock);
-        if (!rx.stationary || u.band.clock_mode == LPK_CLOCK_HOST) {
+        if ((flags & LPK_GEN_DEVICE_CLOCK) && u.band.rx_kind != LPK_RX_PER_SAMPLE) use_device_clock(u.band, rx.clock);
+        if (u.band.rx_kind == LPK_RX_PER_SAMPLE || u.band.clock_mode == LPK_CLOCK_HOST) {
             rest.push_back(w);
             continue;
         }

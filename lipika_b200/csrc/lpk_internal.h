@@ -112,7 +112,7 @@ cudaError_t launch_band_split(int variant, const DevBand &b, const DevTx *d_tx, 
                               double *dbg_delay, cudaStream_t s);
 // True when the band can take the split path (stationary receiver).
 inline bool use_split(const lpk_band_desc *d) {
-    return d->solver == LPK_SOLVER_SPLIT && d->rx_kind == LPK_RX_STATIONARY;
+    return d->solver == LPK_SOLVER_SPLIT && (d->rx_kind == LPK_RX_STATIONARY || d->rx_kind == LPK_RX_KEPLER);
 }
 cudaError_t launch_or_flags(const uint32_t *d_uw, uint8_t *d_unocc, int32_t n_active, int mode, cudaStream_t s);
 // Totals of scan blocks [b_from, b_to).
@@ -129,6 +129,8 @@ cudaError_t launch_walk_materialize(uint64_t seed, double sigma, const double *d
 lpk_status prepare_walk(lpk_ctx *ctx, const lpk_band_desc *d, int64_t i0, int64_t n, DevBand &b, double *d_eps,
                         int64_t eps_cap);
 int64_t walk_span(const lpk_band_desc *d, int64_t i0, int64_t n, int64_t *kA);
+// The device constants of a circular Keplerian orbit (lpk_traj.cu).
+bool make_orbit(const lpk_kepler_orbit &k, DevOrbit &o);
 // Device-clock inputs of a band chunk in one scratch region: the walk
 // values (DEVICE_WALK) followed by the staged flicker points (a flicker
 // track). clock_region_bytes: the region's size (256-byte aligned parts);

@@ -38,17 +38,19 @@ k_band_reference(const DevBand b, const DevTx *__restrict__ txs, const int32_t *
         t_local = __ddiv_rn((double)g, b.fs);  // src/pipeline.rs:918
         delta = band_delta(b, j, t_local);
         tu = __dsub_rn(t_local, delta);         // :927
-        band_rx(b, j, ox, oy, oz);
+        band_rx(b, j, tu, ox, oy, oz);
     }
     // Horizon gate over the block's samples (src/channel/horizon.rs): a
     // transmitter certainly below the antenna cutoff for all of them is
     // skipped; the per-sample path would give it zero gain everywhere.
     __shared__ double red[96];
     __shared__ unsigned char skip[256];
-    const bool gate = b.has_antenna && b.has_cutoff;
+    // (a receiver on an orbit is not gated: the bound needs the block's
+    // receiver positions before the solve; skipping is an optimisation only)
+    const bool gate = b.has_antenna && b.has_cutoff && b.rx_kind != LPK_RX_KEPLER;
     if (gate) {
         double cx, cy, cz;
-        band_rx(b, (int64_t)blockIdx.x * blockDim.x, cx, cy, cz);  // the block's first sample is in the chunk
+        band_rx(b, (int64_t)blockIdx.x * blockDim.x, 0.0, cx, cy, cz);  // the block's first sample is in the chunk
         double lo = live ? tu : __longlong_as_double(0x7ff0000000000000LL);
         double hi = live ? tu : -__longlong_as_double(0x7ff0000000000000LL);
         const double ex = ox - cx, ey = oy - cy, ez = oz - cz;
@@ -111,7 +113,7 @@ k_band_fp64(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__res
     const double delta = band_delta(b, live ? j : 0, t_local);
     const double tu = t_local - delta;
     double ox, oy, oz;
-    band_rx(b, live ? j : 0, ox, oy, oz);
+    band_rx(b, live ? j : 0, tu, ox, oy, oz);
     float acc_re = 0.0f, acc_im = 0.0f;
     for (int k = 0; k < n_active; ++k) {
         float cr = 0.0f, ci = 0.0f;
@@ -142,7 +144,7 @@ k_tx_contribution(const DevBand b, const DevTx *__restrict__ txs, int32_t tx_idx
     double delta = band_delta(b, j, t_local);
     double tu = __dsub_rn(t_local, delta);
     double ox, oy, oz;
-    band_rx(b, j, ox, oy, oz);
+    band_rx(b, j, tu, ox, oy, oz);
     float cr = 0.0f, ci = 0.0f;
     contribution(stx, b, t_local, tu, delta, ox, oy, oz, cr, ci, phase ? phase + j : nullptr,
                  temit ? temit + j : nullptr, range ? range + j : nullptr);

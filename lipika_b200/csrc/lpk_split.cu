@@ -12,6 +12,8 @@ namespace {
 
 // One thread per (tile, transmitter); the block's records are built in
 // shared memory and stored contiguously.
+// MOV: the band's receiver is on an orbit (compiled apart, as the fan-out).
+template <bool MOV>
 __global__ void __launch_bounds__(kAnchorThreads, LPK_ANCHOR_MINB)
 k_split_anchor(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__restrict__ active, int32_t n_active,
                int64_t t0, int64_t n_tiles, int32_t tile_len, AnchorRec *__restrict__ recs,
@@ -23,14 +25,15 @@ k_split_anchor(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__
         const int64_t tile = id / n_active;
         const int k = (int)(id - tile * n_active);
         const int64_t gs = (t0 + tile) * tile_len;  // absolute sample indices of the tile
-        fit_anchor(b, txs[active[k]], gs, gs + tile_len - 1, false, srec[threadIdx.x], exts + id);
+        fit_anchor<MOV>(b, txs[active[k]], gs, gs + tile_len - 1, false, srec[threadIdx.x], exts + id);
     }
     __syncthreads();
     store_recs(srec, recs + base, (int)(total - base < kAnchorThreads ? total - base : kAnchorThreads));
 }
 
-// One block per tile.
-template <int TILE, int THREADS, int MINB, bool DBG, bool UNOCC, bool ACC = false>
+// One block per tile. MOV: the band's receiver is on an orbit (compiled
+// apart, so the stationary kernels carry no receiver-orbit code).
+template <int TILE, int THREADS, int MINB, bool DBG, bool UNOCC, bool ACC, bool MOV>
 __global__ void __launch_bounds__(THREADS, MINB)
 k_band_split(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__restrict__ active, int32_t n_active,
              int64_t t0, const AnchorRec *__restrict__ recs, const AnchorExt *__restrict__ exts,
@@ -43,8 +46,8 @@ k_band_split(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__re
     stage_tile(txs, active, n_active, recs + tile * n_active, stx, srec, true);
     __syncthreads();
     const int64_t first = (t0 + tile) * TILE - b.i0;  // chunk index of the tile's first sample
-    split_tile<TILE / THREADS, THREADS, DBG, UNOCC, ACC>(b, stx, srec, exts + tile * n_active, n_active, first, out,
-                                                         dbg_phase, dbg_temit, dbg_delay);
+    split_tile<TILE / THREADS, THREADS, DBG, UNOCC, ACC, MOV>(b, stx, srec, exts + tile * n_active, n_active, first,
+                                                              out, dbg_phase, dbg_temit, dbg_delay);
 }
 
 using SplitKernel = void (*)(const DevBand, const DevTx *, const int32_t *, int32_t, int64_t, const AnchorRec *,
@@ -52,12 +55,15 @@ using SplitKernel = void (*)(const DevBand, const DevTx *, const int32_t *, int3
 
 struct SplitShape {
     int tile, threads, minb;
-    SplitKernel fast, fast_unocc, dbg, acc;  // acc: accuracy mode (DevBand::acc_stats)
+    SplitKernel fast[2], fast_unocc[2], dbg[2], acc[2];  // [receiver on an orbit]; acc: accuracy mode
 };
 
 #define LPK_SPLIT_ENTRY(I, T, N, M)                                                                              \
-    {T, N, M, k_band_split<T, N, M, false, false>, k_band_split<T, N, M, false, true>,                           \
-     k_band_split<T, N, M, true, false>, k_band_split<T, N, M, false, false, true>},
+    {T, N, M,                                                                                                    \
+     {k_band_split<T, N, M, false, false, false, false>, k_band_split<T, N, M, false, false, false, true>},      \
+     {k_band_split<T, N, M, false, true, false, false>, k_band_split<T, N, M, false, true, false, true>},        \
+     {k_band_split<T, N, M, true, false, false, false>, k_band_split<T, N, M, true, false, false, true>},        \
+     {k_band_split<T, N, M, false, false, true, false>, k_band_split<T, N, M, false, false, true, true>}},
 const SplitShape kShapes[kSplitVariants] = {LPK_SPLIT_VARIANTS(LPK_SPLIT_ENTRY)};
 #undef LPK_SPLIT_ENTRY
 
@@ -88,7 +94,8 @@ cudaError_t launch_split_anchor(int variant, const DevBand &b, const DevTx *d_tx
     if (na <= 0) return cudaSuccess;
     AnchorRec *recs = (AnchorRec *)d_recs;
     AnchorExt *exts = (AnchorExt *)(recs + na);  // 16-byte aligned: sizeof(AnchorRec) is a multiple of 16
-    k_split_anchor<<<(unsigned)((na + kAnchorThreads - 1) / kAnchorThreads), kAnchorThreads, 0, s>>>(
+    (b.rx_kind == LPK_RX_KEPLER ? k_split_anchor<true> : k_split_anchor<false>)<<<
+        (unsigned)((na + kAnchorThreads - 1) / kAnchorThreads), kAnchorThreads, 0, s>>>(
         b, d_tx, d_active, n_active, t0, n_tiles, sh.tile, recs, exts);
     return cudaGetLastError();
 }
@@ -104,7 +111,9 @@ cudaError_t launch_split_fanout(int variant, const DevBand &b, const DevTx *d_tx
     AnchorRec *recs = (AnchorRec *)d_recs;
     AnchorExt *exts = (AnchorExt *)(recs + na);
     const size_t smem = (sizeof(DevTx) + sizeof(AnchorRec)) * (size_t)n_active;
-    SplitKernel kern = b.acc_stats ? sh.acc : (dbg_phase ? sh.dbg : (b.unocc_words ? sh.fast_unocc : sh.fast));
+    const int mov = b.rx_kind == LPK_RX_KEPLER;
+    SplitKernel kern = b.acc_stats ? sh.acc[mov]
+                                   : (dbg_phase ? sh.dbg[mov] : (b.unocc_words ? sh.fast_unocc[mov] : sh.fast[mov]));
     if (smem > 40 * 1024) {  // leaves room for the kernel's static shared arrays
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;

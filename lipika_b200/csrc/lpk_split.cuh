@@ -94,6 +94,10 @@ struct __align__(16) AnchorRec {
     double node0, node1;              // first node of each iterate
     double p0b[3], p1b[3];            // piece 1 of each iterate
     double k1b;                       // second-iterate slope of piece 1
+    // A receiver on an orbit: ∂delay/∂(receiver query time) of the first and
+    // second iterate, linear over the tile (a + b Δ); they carry the
+    // rounding of the receiver's query epoch + tu into the delay.
+    float krx1a, krx1b, krx2a, krx2b;
     double reserved;
 };
 static_assert(sizeof(AnchorRec) % 16 == 0, "AnchorRec arrays must keep 16-byte alignment");
@@ -138,13 +142,18 @@ __device__ __forceinline__ int64_t seg_unrounded(const DevTx &tx, double t, doub
 // the Sagnac angle ω (tu - tq); also ∂delay/∂tq along the segment.
 __device__ __forceinline__ double iterate_unrounded(const DevTx &tx, double tu, double tq, double de, int64_t lo,
                                                     double ox, double oy, double oz, double inv_c, double *range,
-                                                    double *dd_dt) {
+                                                    double *dd_dt, double *los = nullptr) {
     double sx, sy, sz;
     pos_unrounded(tx, tq, de, lo, sx, sy, sz);
     double w = kEarthRate * (tu - tq);
     double dx = sx + w * sy - ox, dy = sy - w * sx - oy, dz = sz - oz;
     double r = sqrt(dx * dx + dy * dy + dz * dz);
     if (range) *range = r;
+    if (los) {  // unit line of sight, receiver to source
+        los[0] = dx / r;
+        los[1] = dy / r;
+        los[2] = dz / r;
+    }
     if (dd_dt) {
         double vx = 0.0, vy = 0.0, vz = 0.0;
         if (tx.traj_kind != 0) {
@@ -203,6 +212,9 @@ constexpr double kSplitInf = __builtin_huge_val();
 // the nodes; the second iterate per piece at the three times serves its fit,
 // k1 (middle) and the ranges at the ends (amplitude). Six evaluations for a
 // tile inside one grid segment.
+// MOV: the band's receiver is on an orbit (positions and velocities at the
+// fit times, line-of-sight slopes for the receiver's query rounding).
+template <bool MOV>
 __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, int64_t gs, int64_t ge, bool exact_only,
                                            AnchorRec &r, AnchorExt *x) {
     const double tls = (double)gs / b.fs, tle = (double)ge / b.fs;
@@ -226,6 +238,7 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
     r.nts = tx.neg_tau_src;
     r.epoch_rel = tx.epoch_rel;
     r.reserved = 0.0;
+    r.krx1a = r.krx1b = r.krx2a = r.krx2b = 0.0f;
     if (exact_only) {
         r.amp0 = r.amp1 = 0.0f;
         r.guard = r.hm = 0.0;
@@ -234,6 +247,18 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
         return;
     }
     const double tu[3] = {tus, tus + h, tue};
+    // the receiver at the fit times (unrounded query: orbit time rx_de + tu)
+    // and its velocity, which the per-sample receiver-rounding terms need
+    double O[3][3], V[3][3], u1[3][3], u2[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        if constexpr (MOV) {
+            kepler_at(b.rx_orb, b.rx_de + tu[i], O[i][0], O[i][1], O[i][2], V[i]);
+            u1[i][0] = u1[i][1] = u1[i][2] = u2[i][0] = u2[i][1] = u2[i][2] = 0.0;
+        } else {
+            O[i][0] = ox; O[i][1] = oy; O[i][2] = oz;
+        }
+    }
     double d0[3];
     int64_t l0[3] = {0, 0, 0}, l1[3] = {0, 0, 0};
     bool exact = false;
@@ -245,7 +270,8 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
             l0[i] = seg_unrounded(tx, tq, de, cl);
             exact |= cl;
         }
-        d0[i] = iterate_unrounded(tx, tu[i], tq, de, l0[i], ox, oy, oz, b.inv_c, nullptr, i == 1 ? &r.k0 : nullptr);
+        d0[i] = iterate_unrounded(tx, tu[i], tq, de, l0[i], O[i][0], O[i][1], O[i][2], b.inv_c, nullptr,
+                                  i == 1 ? &r.k0 : nullptr, MOV ? u1[i] : nullptr);
         if (tx.traj_kind != 0) {
             l1[i] = seg_unrounded(tx, tu[i] - d0[i], de, cl);
             exact |= cl;
@@ -276,8 +302,8 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
 #pragma unroll
             for (int i = 0; i < 3; ++i)
                 v[i] = l0[0] + p == l0[i] ? d0[i]
-                                          : iterate_unrounded(tx, tu[i], tu[i] - kEmissionLag, de, l0[0] + p, ox, oy,
-                                                              oz, b.inv_c, nullptr, nullptr);
+                                          : iterate_unrounded(tx, tu[i], tu[i] - kEmissionLag, de, l0[0] + p, O[i][0],
+                                                              O[i][1], O[i][2], b.inv_c, nullptr, nullptr);
             quad3(v[0], v[1], v[2], h, ih, p == 0 ? r.p0 : (p == 1 ? r.p0b : x->p0[p - 2]));
         }
         for (int64_t p = 0; p <= n1; ++p) {
@@ -285,8 +311,9 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 double *range = (i == 0 && p == 0) ? &rs : ((i == 2 && p == n1) ? &re : nullptr);
-                v[i] = iterate_unrounded(tx, tu[i], tu[i] - d0[i], de, l1[0] + p, ox, oy, oz, b.inv_c, range,
-                                         i == 1 ? &k1 : nullptr);
+                v[i] = iterate_unrounded(tx, tu[i], tu[i] - d0[i], de, l1[0] + p, O[i][0], O[i][1], O[i][2], b.inv_c,
+                                         range, i == 1 ? &k1 : nullptr,
+                                         (MOV && l1[0] + p == l1[i]) ? u2[i] : nullptr);
             }
             if (l1[0] + p == l1[1]) d1m = v[1];  // the second iterate on its natural segment at the middle
             if (p == 0) r.k1 = k1; else if (p == 1) r.k1b = k1; else x->k1[p - 2] = k1;
@@ -294,6 +321,25 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
         }
         te_s = tus - poly2(r.p1, 0.0);
         te_e = tue - poly2(n1 == 0 ? r.p1 : (n1 == 1 ? r.p1b : x->p1[n1 - 2]), 2.0 * h);
+    }
+    // a receiver on an orbit: its query epoch + tu rounds like the
+    // transmitter queries; krx = -(line of sight · receiver velocity) / c of
+    // each iterate, linear over the tile. With an antenna, or where the
+    // orbit time of the rounded query would round again, the tile is exact.
+    r.krx1a = r.krx1b = r.krx2a = r.krx2b = 0.0f;
+    if constexpr (MOV) {
+        if (b.has_antenna || !b.rx_split_ok) exact = true;
+        double kr[2][2];
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int i = 2 * e;
+            kr[0][e] = -(u1[i][0] * V[i][0] + u1[i][1] * V[i][1] + u1[i][2] * V[i][2]) * b.inv_c;
+            kr[1][e] = -(u2[i][0] * V[i][0] + u2[i][1] * V[i][1] + u2[i][2] * V[i][2]) * b.inv_c;
+        }
+        r.krx1a = (float)kr[0][0];
+        r.krx1b = (float)((kr[0][1] - kr[0][0]) * (0.5 * ih));
+        r.krx2a = (float)kr[1][0];
+        r.krx2b = (float)((kr[1][1] - kr[1][0]) * (0.5 * ih));
     }
     float amp_s = (float)(tx.amp_factor / rs), amp_e = (float)(tx.amp_factor / re);
     if (!exact && b.has_antenna) {
@@ -415,9 +461,10 @@ __device__ __forceinline__ int64_t tile_sample(int64_t first, int s) {
 // and psi = -2π f_lo Δt reduced modulo 2π. The carrier phase
 // -2π f (delay + Δt) + 2π (f - f_lo) t_local equals
 // -2π f delay + 2π (f - f_lo) tu - 2π f_lo Δt (t_local = tu + Δt), so the
-// part that depends on Δt alone is formed once per sample.
+// part that depends on Δt alone is formed once per sample. qr: the rounding
+// offset of the receiver's query epoch + tu (a receiver on an orbit only).
 struct SampleCtx {
-    double tu, d, q0, psi;
+    double tu, d, q0, psi, qr;
 };
 
 // t_local and Δt of sample s of this thread (src/pipeline.rs:918-927): the
@@ -525,7 +572,9 @@ __device__ __forceinline__ void split_baseband(const DevTx &tx, const AnchorRec 
 // arithmetic (the exact path's solve and phase) and the largest delay and
 // carrier-phase differences are kept in acc[0], acc[1]; acc[2] counts the
 // fast-path samples compared.
-template <int K, bool DBG, int NK, int S, int THREADS, bool ACC = false>
+// MOV: a receiver on an orbit: the rounding of its query time enters both
+// iterates through the record's krx slopes.
+template <int K, bool DBG, int NK, int S, int THREADS, bool ACC = false, bool MOV = false>
 __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, const AnchorExt *X, double epoch,
                                            const SampleCtx *sc,
                                            unsigned fit, float *ar, float *ai, unsigned &redo, int64_t first,
@@ -557,7 +606,12 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
         } else {
             t1s = tu - fma(d, fma(d, a2, a1), a0);
         }
-        const double t1r = fma(-k0, c.q0, t1s);  // the reference's t1
+        double t1r = fma(-k0, c.q0, t1s);  // the reference's t1
+        float df = 0.0f;
+        if constexpr (MOV) {
+            df = __double2float_rn(d);
+            t1r = fma(-(double)__fmaf_rn(R.krx1b, df, R.krx1a), c.qr, t1r);
+        }
         const double s1 = __dadd_rn(epoch, t1r);  // its second query
         const double e1 = __dsub_rn(s1, epoch);
         bool ok = fabs(e1 - t1r) < hm;
@@ -578,7 +632,8 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
             poly1 = fma(d, fma(d, b2, b1), b0);
             k1 = ka;
         }
-        const double delay = fma(k1, e1 - t1s, poly1);
+        double delay = fma(k1, e1 - t1s, poly1);
+        if constexpr (MOV) delay = fma((double)__fmaf_rn(R.krx2b, df, R.krx2a), c.qr, delay);
         const double te = tu - delay;
         float bre, bim;
         double rb = 0.0;
@@ -635,8 +690,9 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
                 const DevBand &b = *acc_band;
                 double tl, dl;
                 sample_clock<THREADS>(b, first, s, __drcp_rn(b.fs), tl, dl);
-                double te_ref, r_ref;
-                solve_reference(tx, tu, b.rx[0], b.rx[1], b.rx[2], epoch, 2, b.inv_c, te_ref, r_ref);
+                double te_ref, r_ref, rox, roy, roz;
+                band_rx(b, 0, tu, rox, roy, roz);
+                solve_reference(tx, tu, rox, roy, roz, epoch, 2, b.inv_c, te_ref, r_ref);
                 const double delay_ref = __dmul_rn(r_ref, b.inv_c);
                 const double tif = __dmul_rn(kTau, __dsub_rn(tx.carrier, b.lo));
                 const double ph_ref = __dadd_rn(__dmul_rn(tx.neg_tau_src, __dadd_rn(delay_ref, dl)),
@@ -672,7 +728,9 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
 // differences go to b.acc_stats[0..1] (atomic max on the bit patterns of
 // non-negative doubles), its fast-path and exact-path (sample, transmitter)
 // counts are added to b.acc_stats[2..3].
-template <int S, int THREADS, bool DBG, bool UNOCC, bool ACC = false>
+// MOV: the band's receiver is on an orbit (see split_pass); its horizon gate
+// is off (an optimisation only: the gated samples are zero either way).
+template <int S, int THREADS, bool DBG, bool UNOCC, bool ACC, bool MOV>
 // xrec: the tile's AnchorExt records in global memory (index k per
 // transmitter), read only for tiles that cross more than one grid node.
 __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, const AnchorRec *srec,
@@ -702,7 +760,12 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
         const double tu = __dsub_rn(tl, dl);                      // :927
         const double t0q = __dsub_rn(tu, kEmissionLag);
         const double s0 = __dadd_rn(b.epoch, t0q);
-        sc[s] = SampleCtx{tu, tu - tu0, __dsub_rn(__dsub_rn(s0, b.epoch), t0q), reduce_2pi(nlo * dl)};
+        double qr = 0.0;
+        if constexpr (MOV) {  // the receiver's query epoch + tu, rounded like s0
+            const double sr = __dadd_rn(b.epoch, tu);
+            qr = __dsub_rn(__dsub_rn(sr, b.epoch), tu);
+        }
+        sc[s] = SampleCtx{tu, tu - tu0, __dsub_rn(__dsub_rn(s0, b.epoch), t0q), reduce_2pi(nlo * dl), qr};
         live |= (unsigned)lv << s;
         // the fit range depends only on the tile: the same for every
         // transmitter (the pass sees `fit & live`: a sample outside the
@@ -714,7 +777,7 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
     // the tile adds nothing (the exact path would give it zero gain).
     __shared__ double gate_red[96];
     __shared__ unsigned char gate_skip[256];
-    const bool hgate = b.has_antenna && b.has_cutoff;  // uniform over the block
+    const bool hgate = !MOV && b.has_antenna && b.has_cutoff;  // uniform over the block
     if (hgate) {
         double lo = __longlong_as_double(0x7ff0000000000000LL), hi = -lo, r2 = 0.0;
         bool fin = true;
@@ -756,13 +819,13 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
 #define LPK_PASS(KIND)                                                                                           \
     do {                                                                                                         \
         if (nk == 0)                                                                                             \
-            split_pass<KIND, DBG, 0, S, THREADS, ACC>(T, R, xrec + k, b.epoch, sc, fit & live, ar, ai, redo, first,  \
+            split_pass<KIND, DBG, 0, S, THREADS, ACC, MOV>(T, R, xrec + k, b.epoch, sc, fit & live, ar, ai, redo, first,  \
                                                       dbg_phase, dbg_temit, dbg_delay, &b, acc);                  \
         else if (nk == 1)                                                                                        \
-            split_pass<KIND, DBG, 1, S, THREADS, ACC>(T, R, xrec + k, b.epoch, sc, fit & live, ar, ai, redo, first,  \
+            split_pass<KIND, DBG, 1, S, THREADS, ACC, MOV>(T, R, xrec + k, b.epoch, sc, fit & live, ar, ai, redo, first,  \
                                                       dbg_phase, dbg_temit, dbg_delay, &b, acc);                  \
         else                                                                                                     \
-            split_pass<KIND, DBG, kSplitNodes, S, THREADS, ACC>(T, R, xrec + k, b.epoch, sc, fit & live, ar, ai,     \
+            split_pass<KIND, DBG, kSplitNodes, S, THREADS, ACC, MOV>(T, R, xrec + k, b.epoch, sc, fit & live, ar, ai,     \
                                                                 redo, first, dbg_phase, dbg_temit, dbg_delay, &b,  \
                                                                 acc);                                             \
     } while (0)
@@ -789,7 +852,9 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
             float cr = 0.0f, ci = 0.0f;
             double ph = 0.0, te = 0.0, rg = 0.0, tl, dl;
             sample_clock<THREADS>(b, first, s, rfs, tl, dl);
-            const bool on = contribution(T, b, tl, sc[s].tu, dl, b.rx[0], b.rx[1], b.rx[2], cr, ci, &ph, &te, &rg);
+            double ox = b.rx[0], oy = b.rx[1], oz = b.rx[2];
+            if constexpr (MOV) band_rx(b, 0, sc[s].tu, ox, oy, oz);
+            const bool on = contribution(T, b, tl, sc[s].tu, dl, ox, oy, oz, cr, ci, &ph, &te, &rg);
             if constexpr (UNOCC) {
                 if (on && !gate_off) atomicOr(b.unocc_words + k, 1u);
             } else {

@@ -21,10 +21,6 @@ namespace {
 
 constexpr double kKeplerGm = 3.986005e14;  // src/geometry/kepler.rs:12
 
-struct DevOrbit {
-    double r, mm, nu0, si, ci, so, co, epoch;
-};
-
 __global__ void __launch_bounds__(256)
 k_kepler_table(const DevOrbit *__restrict__ orbits, int32_t n_orbits, double t0, double dt, int64_t n,
                double *__restrict__ out) {
@@ -35,25 +31,33 @@ k_kepler_table(const DevOrbit *__restrict__ orbits, int32_t n_orbits, double t0,
         const int64_t i = id - (int64_t)o * n;
         const DevOrbit k = orbits[o];
         const double t = __dadd_rn(t0, __dmul_rn((double)i, dt));  // start + i·dt (precomputed.rs)
-        const double e = __dsub_rn(t, k.epoch);
-        const double nu = __dadd_rn(k.nu0, __dmul_rn(k.mm, e));
-        const double snu = sin(nu), cnu = cos(nu);
-        const double xp = __dmul_rn(k.r, cnu), yp = __dmul_rn(k.r, snu);
-        const double y1 = __dmul_rn(yp, k.ci), z1 = __dmul_rn(yp, k.si);
-        const double xe = __dsub_rn(__dmul_rn(xp, k.co), __dmul_rn(y1, k.so));
-        const double ye = __dadd_rn(__dmul_rn(xp, k.so), __dmul_rn(y1, k.co));
-        const double th = __dmul_rn(kEarthRate, e);
-        const double s = sin(th), c = cos(th);
+        double x, y, z;
+        kepler_at(k, __dsub_rn(t, k.epoch), x, y, z);
         double *dst = out + (int64_t)o * 3 * n;
-        dst[i] = __dadd_rn(__dmul_rn(xe, c), __dmul_rn(ye, s));
-        dst[n + i] = __dadd_rn(__dmul_rn(-xe, s), __dmul_rn(ye, c));
-        dst[2 * n + i] = z1;
+        dst[i] = x;
+        dst[n + i] = y;
+        dst[2 * n + i] = z;
     }
 }
 
 inline double deg2rad(double deg) { return deg * (M_PI / 180.0); }  // f64::to_radians
 
 }  // namespace
+
+// The per-orbit part of kepler.rs:32-85 with the host's libm (the order of
+// the host's kepler() in lpk_host.cpp); false for a non-positive or
+// non-finite radius or a non-finite angle or epoch.
+bool make_orbit(const lpk_kepler_orbit &k, DevOrbit &o) {
+    const double r = k.semi_major_axis_m;
+    if (!(r > 0.0) || !std::isfinite(r) || !std::isfinite(k.inclination_deg) || !std::isfinite(k.raan_deg) ||
+        !std::isfinite(k.true_anomaly_deg_at_epoch) || !std::isfinite(k.epoch_unix))
+        return false;
+    const double inc = deg2rad(k.inclination_deg), om = deg2rad(k.raan_deg);
+    o = DevOrbit{r, std::sqrt(kKeplerGm / (r * r * r)), deg2rad(k.true_anomaly_deg_at_epoch), std::sin(inc),
+                 std::cos(inc), std::sin(om), std::cos(om), k.epoch_unix};
+    return true;
+}
+
 }  // namespace lpk
 
 using namespace lpk;
@@ -68,20 +72,8 @@ extern "C" lpk_status lpk_kepler_tables(lpk_ctx *c, const lpk_kepler_orbit *orbi
         return fail(c, LPK_EINVAL, "t0 must be finite and dt positive");
     if (n_points > ((int64_t)1 << 31)) return fail(c, LPK_EINVAL, "too many grid points");
     std::vector<DevOrbit> h((size_t)n_orbits);
-    for (int32_t o = 0; o < n_orbits; ++o) {  // the per-orbit part of kepler.rs:32-85, host libm
-        const lpk_kepler_orbit &k = orbits[o];
-        const double r = k.semi_major_axis_m;
-        if (!(r > 0.0) || !std::isfinite(r)) return fail(c, LPK_EINVAL, "semi-major axis must be positive");
-        const double inc = deg2rad(k.inclination_deg), om = deg2rad(k.raan_deg);
-        h[o] = DevOrbit{r,
-                        std::sqrt(kKeplerGm / (r * r * r)),
-                        deg2rad(k.true_anomaly_deg_at_epoch),
-                        std::sin(inc),
-                        std::cos(inc),
-                        std::sin(om),
-                        std::cos(om),
-                        k.epoch_unix};
-    }
+    for (int32_t o = 0; o < n_orbits; ++o)
+        if (!make_orbit(orbits[o], h[o])) return fail(c, LPK_EINVAL, "bad orbit (radius must be positive)");
     cudaSetDevice(c->device);
     const size_t obytes = sizeof(DevOrbit) * (size_t)n_orbits;
     const size_t gbytes = sizeof(double) * 3 * (size_t)n_points * (size_t)n_orbits;

@@ -26,7 +26,7 @@ LPK_ENOTSUP = -6
 
 LPK_TX_TRAJ_STATIONARY, LPK_TX_TRAJ_PRECOMPUTED = 0, 1
 LPK_CLOCK_HOST, LPK_CLOCK_DETERMINISTIC, LPK_CLOCK_DEVICE_WALK = 0, 1, 2
-LPK_RX_STATIONARY, LPK_RX_PER_SAMPLE = 0, 1
+LPK_RX_STATIONARY, LPK_RX_PER_SAMPLE, LPK_RX_KEPLER = 0, 1, 2
 LPK_POST_GAIN, LPK_POST_NONLINEARITY, LPK_POST_ADC = 0, 1, 2
 LPK_SOLVER_REFERENCE, LPK_SOLVER_SPLIT, LPK_SOLVER_FP64_TUNED = 0, 1, 2
 LPK_NOISE_OFF, LPK_NOISE_ON, LPK_GEN_DEVICE_CLOCK, LPK_GEN_SPLIT, LPK_GEN_AUTOTUNE = 0, 1, 2, 4, 8
@@ -70,6 +70,11 @@ class PostOp(C.Structure):
     _fields_ = [("kind", C.c_int32), ("bits", C.c_uint32), ("param", C.c_double)]
 
 
+class KeplerOrbit(C.Structure):
+    _fields_ = [("semi_major_axis_m", C.c_double), ("inclination_deg", C.c_double), ("raan_deg", C.c_double),
+                ("true_anomaly_deg_at_epoch", C.c_double), ("epoch_unix", C.c_double)]
+
+
 class BandDesc(C.Structure):
     _fields_ = [
         ("epoch_unix", C.c_double), ("fs_hz", C.c_double), ("lo_hz", C.c_double),
@@ -85,6 +90,7 @@ class BandDesc(C.Structure):
         ("n_post", C.c_int32), ("solver", C.c_int32),
         ("post", PostOp * 3),
         ("flicker_delta_s", C.POINTER(C.c_double)), ("flicker_n", C.c_int64),
+        ("rx_orbit", KeplerOrbit),
     ]
 
 
@@ -96,11 +102,6 @@ class BandResult(C.Structure):
 class WorkUnit(C.Structure):
     _fields_ = [("band", BandDesc), ("active", C.POINTER(C.c_int32)), ("n_active", C.c_int32),
                 ("reserved", C.c_int32), ("n_samples", C.c_int64)]
-
-
-class KeplerOrbit(C.Structure):
-    _fields_ = [("semi_major_axis_m", C.c_double), ("inclination_deg", C.c_double), ("raan_deg", C.c_double),
-                ("true_anomaly_deg_at_epoch", C.c_double), ("epoch_unix", C.c_double)]
 
 
 SINK_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.POINTER(CF32), C.c_int64)

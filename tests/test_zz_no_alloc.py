@@ -5,7 +5,7 @@ device through its own pool, cannot let the library call cudaMalloc while it
 renders. The static entry point keeps its working memory in one file-scope
 device array instead; these checks call it through the C ABI and compare it
 with lpk_band_chunk_device, chunk after chunk, for both solvers, with a
-flicker clock and with an antenna (the array keeps the previous call's contents, so the second call
+flicker clock, with an orbiting receiver and with an antenna (the array keeps the previous call's contents, so the second call
 shows nothing stale leaks through), and time the walk rebuild it does on
 every call.
 This file is collected last on purpose.
@@ -83,6 +83,23 @@ def test_static_scratch_flicker_clock_both_solvers():
     for solver in (N.LPK_SOLVER_REFERENCE, N.LPK_SOLVER_SPLIT):
         d.solver = solver
         _compare_two_calls(ctx, prep, d, 0, 1, 400_000, (2_000_000, 77_777), lambda k: [1] * k)
+    prep.close()
+    ctx.close()
+
+
+def test_static_scratch_orbiting_receiver_both_solvers():
+    """A receiver on a circular Keplerian orbit (positions on the device)."""
+    from lipika_b200 import workloads as W
+    ctx = N.Context(0)
+    sc = scenes.config_c1(duration_s=2.0)
+    sc.receivers[0].trajectory = W._kepler(6_900_000.0, 60.0, 30.0, 100.0)
+    prep = P.Prepared(sc, ctx)
+    d = prep.band_desc(0, 1, 2026, 1)
+    d.clock_mode = N.LPK_CLOCK_DEVICE_WALK
+    assert d.rx_kind == N.LPK_RX_KEPLER
+    for solver in (N.LPK_SOLVER_REFERENCE, N.LPK_SOLVER_SPLIT):
+        d.solver = solver
+        _compare_two_calls(ctx, prep, d, 0, 1, 300_000, (1_500_000, 31_337), lambda k: [1] * k)
     prep.close()
     ctx.close()
 
