@@ -254,7 +254,7 @@ lpk_status lpk_split_accuracy(lpk_ctx *ctx, const lpk_band_desc *band, const int
  * they render (a real-time thread that must not stall on the CUDA allocator,
  * a host that reserved the device for its own pool). No counterpart in the
  * reference. It calls no cudaMalloc/cudaFree: its working memory is one
- * file-scope static device array of 22 MiB that every GPU loading this
+ * file-scope static device array of 22.6 MiB that every GPU loading this
  * library holds until exit. It runs the kernels lpk_band_chunk_device runs
  * for the band's solver (the split path for LPK_SOLVER_SPLIT with a
  * stationary receiver, the FP64 kernel otherwise) on the same inputs, so

@@ -38,10 +38,11 @@ constexpr size_t kOffCarry = kOffTotals + sizeof(double) * kMaxWalkBlocks;
 constexpr size_t kOffGsum = kOffCarry + sizeof(double) * (kMaxWalkBlocks + 1);
 constexpr size_t kOffEps = (kOffGsum + sizeof(double) * (kMaxWalkBlocks / lpk::kGroupBlocks + 1) + 255) / 256 * 256;
 constexpr size_t kOffRecs = (kOffEps + sizeof(double) * kMaxWalkSpan + 255) / 256 * 256;
-constexpr size_t kMaxRecsBytes = size_t(12) << 20;  // split anchor records: 32,768 (tile, transmitter) pairs
+constexpr size_t kMaxRecsBytes = size_t(32768) * 400;  // split anchor records: 32,768 (tile, transmitter) pairs
+                                                       // of 240 + 160 bytes (record + extension)
 constexpr size_t kOffFlicker = kOffRecs + kMaxRecsBytes;
 constexpr int64_t kMaxFlicker = 8192;             // flicker track points one chunk may read (64 s)
-constexpr size_t kStaticBytes = kOffFlicker + sizeof(double) * kMaxFlicker;  // 22.1 MiB
+constexpr size_t kStaticBytes = kOffFlicker + sizeof(double) * kMaxFlicker;  // 22.6 MiB
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
 

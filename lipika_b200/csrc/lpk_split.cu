@@ -8,6 +8,9 @@
 
 namespace lpk {
 
+static_assert(sizeof(AnchorRec) + sizeof(AnchorExt) == 400,
+              "lpk_band_chunk_device_static sizes its record area for 400-byte (record, extension) pairs");
+
 namespace {
 
 // One thread per (tile, transmitter); the block's records are built in

@@ -95,12 +95,13 @@ struct __align__(16) AnchorRec {
     double p0b[3], p1b[3];            // piece 1 of each iterate
     double k1b;                       // second-iterate slope of piece 1
     // A receiver on an orbit: ∂delay/∂(receiver query time) of the first and
-    // second iterate, linear over the tile (a + b Δ); they carry the
-    // rounding of the receiver's query epoch + tu into the delay.
-    float krx1a, krx1b, krx2a, krx2b;
-    double reserved;
+    // second iterate at the tile's fit origin (their changes over the tile,
+    // krx1b / krx2b, are in the tile's AnchorExt); they carry the rounding of
+    // the receiver's query epoch + tu into the delay.
+    float krx1a, krx2a;
 };
 static_assert(sizeof(AnchorRec) % 16 == 0, "AnchorRec arrays must keep 16-byte alignment");
+static_assert(sizeof(AnchorRec) == 240, "a bigger record costs the anchor kernels an SM's worth of occupancy");
 static_assert(offsetof(AnchorRec, tu0) == 144 && offsetof(AnchorRec, amp0) == 112,
               "the fast pass's fields fill the record's first 144 bytes");
 
@@ -110,6 +111,8 @@ struct __align__(16) AnchorExt {
     double node0[2], node1[2];        // second and third nodes
     double p0[2][3], p1[2][3];        // pieces 2-3
     double k1[2];
+    float krx1b, krx2b;               // receiver on an orbit: d(krx1a, krx2a)/dΔ (written for every such tile)
+    double reserved;
 };
 
 // Lerp position at epoch-relative time t with the segment forced to `lo`
@@ -237,8 +240,7 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
     r.chip_m0 = 0;
     r.nts = tx.neg_tau_src;
     r.epoch_rel = tx.epoch_rel;
-    r.reserved = 0.0;
-    r.krx1a = r.krx1b = r.krx2a = r.krx2b = 0.0f;
+    r.krx1a = r.krx2a = 0.0f;
     if (exact_only) {
         r.amp0 = r.amp1 = 0.0f;
         r.guard = r.hm = 0.0;
@@ -326,7 +328,6 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
     // transmitter queries; krx = -(line of sight · receiver velocity) / c of
     // each iterate, linear over the tile. With an antenna, or where the
     // orbit time of the rounded query would round again, the tile is exact.
-    r.krx1a = r.krx1b = r.krx2a = r.krx2b = 0.0f;
     if constexpr (MOV) {
         if (b.has_antenna || !b.rx_split_ok) exact = true;
         double kr[2][2];
@@ -337,9 +338,9 @@ __device__ __forceinline__ void fit_anchor(const DevBand &b, const DevTx &tx, in
             kr[1][e] = -(u2[i][0] * V[i][0] + u2[i][1] * V[i][1] + u2[i][2] * V[i][2]) * b.inv_c;
         }
         r.krx1a = (float)kr[0][0];
-        r.krx1b = (float)((kr[0][1] - kr[0][0]) * (0.5 * ih));
+        x->krx1b = (float)((kr[0][1] - kr[0][0]) * (0.5 * ih));
         r.krx2a = (float)kr[1][0];
-        r.krx2b = (float)((kr[1][1] - kr[1][0]) * (0.5 * ih));
+        x->krx2b = (float)((kr[1][1] - kr[1][0]) * (0.5 * ih));
     }
     float amp_s = (float)(tx.amp_factor / rs), amp_e = (float)(tx.amp_factor / re);
     if (!exact && b.has_antenna) {
@@ -610,7 +611,7 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
         float df = 0.0f;
         if constexpr (MOV) {
             df = __double2float_rn(d);
-            t1r = fma(-(double)__fmaf_rn(R.krx1b, df, R.krx1a), c.qr, t1r);
+            t1r = fma(-(double)__fmaf_rn(X->krx1b, df, R.krx1a), c.qr, t1r);
         }
         const double s1 = __dadd_rn(epoch, t1r);  // its second query
         const double e1 = __dsub_rn(s1, epoch);
@@ -633,7 +634,7 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
             k1 = ka;
         }
         double delay = fma(k1, e1 - t1s, poly1);
-        if constexpr (MOV) delay = fma((double)__fmaf_rn(R.krx2b, df, R.krx2a), c.qr, delay);
+        if constexpr (MOV) delay = fma((double)__fmaf_rn(X->krx2b, df, R.krx2a), c.qr, delay);
         const double te = tu - delay;
         float bre, bim;
         double rb = 0.0;
