@@ -50,6 +50,7 @@ struct RoundUnit {
     int64_t i0, n;          // band samples [i0, i0 + n)
     int64_t t0, n_tiles;    // absolute index of the first tile, tile count
     int64_t tile_off, rec_off;  // prefix over schedule slots
+    int64_t grp_off;            // prefix of anchor groups (lpk_split.cuh) over schedule slots
     int32_t unit, pad;
 };
 struct RoundWalk {
@@ -57,7 +58,7 @@ struct RoundWalk {
     int64_t g_known;        // groups whose sums are stored before the round
 };
 struct RoundDesc {
-    int64_t total_tiles, total_recs, total_walk_blocks;
+    int64_t total_tiles, total_recs, total_groups, total_walk_blocks;
     int32_t n_slots, n_walks, tile, parity;  // parity: which output buffer the round writes
     int64_t wb_off[kMaxWalks + 1];  // prefix of scanned blocks per walk
     RoundWalk w[kMaxWalks];
@@ -73,11 +74,11 @@ __device__ __forceinline__ int find_slot_tiles(const RoundDesc &rd, int64_t g) {
     return lo;
 }
 
-__device__ __forceinline__ int find_slot_recs(const RoundDesc &rd, int64_t g) {
+__device__ __forceinline__ int find_slot_groups(const RoundDesc &rd, int64_t g) {
     int lo = 0, hi = rd.n_slots - 1;
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
-        if (rd.s[mid].rec_off <= g) lo = mid; else hi = mid - 1;
+        if (rd.s[mid].grp_off <= g) lo = mid; else hi = mid - 1;
     }
     return lo;
 }
@@ -142,9 +143,12 @@ k_batch_carry(const DevWalk *__restrict__ walks, const RoundDesc *__restrict__ r
         walk_group_carries(dw.totals, dw.gsum, known, rw.bA, rw.bB, g, false, dw.carry, sh);
 }
 
-// Anchor fits of every (slot, tile, transmitter) of the round, one per
-// thread; each block builds its run of records in shared memory and stores
-// it contiguously.
+// Anchor fits of every (slot, tile, transmitter) of the round by anchor
+// groups (lpk_split.cuh): a block takes up to 32 tiles (one per lane) of up
+// to 4 transmitters (one per warp) of one unit, stages the group's
+// transmitters in shared memory (the band's fields are block-uniform reads),
+// fits, and stores the records tile-major. The block's shared memory stays
+// within the carveout that keeps five blocks per SM.
 // MOV: some unit's receiver is on an orbit (compiled apart, as the fan-out).
 template <bool MOV>
 __global__ void __launch_bounds__(kAnchorThreads, LPK_ANCHOR_MINB)
@@ -152,30 +156,37 @@ k_batch_anchor(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ 
                const DevTx *__restrict__ txs, const int32_t *__restrict__ act, const RoundDesc *__restrict__ rd,
                AnchorRec *__restrict__ recs, AnchorExt *__restrict__ exts) {
     __shared__ __align__(16) AnchorRec srec[kAnchorThreads];
-    const int64_t total = rd->total_recs;
+    __shared__ __align__(16) DevTx stx[kAnchorGroupTx];
+    __shared__ int s_slot;
     const int tile_len = rd->tile;
-    for (int64_t base = (int64_t)blockIdx.x * kAnchorThreads; base < total;
-         base += (int64_t)gridDim.x * kAnchorThreads) {
-        const int64_t id = base + threadIdx.x;
-        if (id < total) {
-            const int sl = find_slot_recs(*rd, id);
-            const RoundUnit &ru = rd->s[sl];
-            const BatchUnit bu = units[ru.unit];
-            const int64_t local = id - ru.rec_off;
-            const int64_t tile = local / bu.n_active;
-            const int k = (int)(local - tile * bu.n_active);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int64_t g = blockIdx.x; g < rd->total_groups; g += gridDim.x) {
+        if (threadIdx.x == 0) s_slot = find_slot_groups(*rd, g);
+        __syncthreads();
+        const RoundUnit &ru = rd->s[s_slot];
+        const BatchUnit bu = units[ru.unit];
+        const int64_t ntg = (ru.n_tiles + kAnchorGroupTiles - 1) / kAnchorGroupTiles, local = g - ru.grp_off;
+        const int64_t tile0 = (local % ntg) * kAnchorGroupTiles;
+        const int k0 = (int)(local / ntg) * kAnchorGroupTx;
+        const int nt = (int)(ru.n_tiles - tile0 < kAnchorGroupTiles ? ru.n_tiles - tile0 : kAnchorGroupTiles);
+        const int nk = bu.n_active - k0 < kAnchorGroupTx ? bu.n_active - k0 : kAnchorGroupTx;
+        const DevBand &sb = bands[ru.unit];
+        stage_group_txs(txs, act + bu.act_off + k0, nk, stx);
+        __syncthreads();
+        if (lane < nt && w < nk) {
+            const int64_t tile = tile0 + lane;
             const int64_t gs = (ru.t0 + tile) * tile_len;
-            const DevBand &band = bands[ru.unit];
-            if (MOV && band.rx_kind == LPK_RX_KEPLER)
-                fit_anchor<true>(band, txs[act[bu.act_off + k]], gs, gs + tile_len - 1, bu.exact_only != 0,
-                                 srec[threadIdx.x], exts + id);
+            AnchorExt *x = exts + ru.rec_off + tile * bu.n_active + k0 + w;
+            if (MOV && sb.rx_kind == LPK_RX_KEPLER)
+                fit_anchor<true>(sb, stx[w], gs, gs + tile_len - 1, bu.exact_only != 0,
+                                 srec[lane * kAnchorGroupTx + w], x);
             else
-                fit_anchor<false>(band, txs[act[bu.act_off + k]], gs, gs + tile_len - 1, bu.exact_only != 0,
-                                  srec[threadIdx.x], exts + id);
+                fit_anchor<false>(sb, stx[w], gs, gs + tile_len - 1, bu.exact_only != 0,
+                                  srec[lane * kAnchorGroupTx + w], x);
         }
         __syncthreads();
-        store_recs(srec, recs + base, (int)(total - base < kAnchorThreads ? total - base : kAnchorThreads));
-        __syncthreads();  // srec is rewritten by the next run
+        store_group(srec, recs + ru.rec_off + tile0 * bu.n_active + k0, nt, nk, bu.n_active);
+        __syncthreads();  // srec and stx are rewritten by the next group
     }
 }
 
@@ -349,7 +360,7 @@ void plan_round(lpk_batch *b, int64_t round, int tile, RoundDesc &rd, bool commi
         return (double)n * (double)(b->units[u].n_active + 1);
     };
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost(x) > cost(y); });
-    int64_t tiles = 0, recs = 0;
+    int64_t tiles = 0, recs = 0, groups = 0;
     std::vector<int64_t> kA(b->walks.size(), INT64_MAX), kB(b->walks.size(), -1);
     for (size_t sl = 0; sl < order.size(); ++sl) {
         const int u = order[sl];
@@ -360,9 +371,12 @@ void plan_round(lpk_batch *b, int64_t round, int tile, RoundDesc &rd, bool commi
         ru.n_tiles = (ru.i0 + ru.n - 1) / tile - ru.t0 + 1;
         ru.tile_off = tiles;
         ru.rec_off = recs;
+        ru.grp_off = groups;
         ru.unit = u;
         tiles += ru.n_tiles;
         recs += ru.n_tiles * uh.n_active;
+        groups += (ru.n_tiles + kAnchorGroupTiles - 1) / kAnchorGroupTiles *
+                  ((uh.n_active + kAnchorGroupTx - 1) / kAnchorGroupTx);
         if (uh.walk >= 0) {
             int64_t a;
             int64_t span = walk_span(&uh.desc, ru.i0, ru.n, &a);
@@ -373,6 +387,7 @@ void plan_round(lpk_batch *b, int64_t round, int tile, RoundDesc &rd, bool commi
     rd.n_slots = (int32_t)order.size();
     rd.total_tiles = tiles;
     rd.total_recs = recs;
+    rd.total_groups = groups;
     rd.n_walks = (int32_t)b->walks.size();
     int64_t wb = 0, partial_blocks = 0;
     for (size_t w = 0; w < b->walks.size(); ++w) {

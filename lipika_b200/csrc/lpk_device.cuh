@@ -130,6 +130,7 @@ struct DevBand {
                                         // the scene, so the split path's smooth receiver model holds
     int32_t rx_reserved;
 };
+static_assert(sizeof(DevBand) % 8 == 0, "DevBand is staged in 8-byte words");
 
 // ---------------------------------------------------------------- helpers
 // Read-only load of one 32-byte grid point as two 16-byte loads.

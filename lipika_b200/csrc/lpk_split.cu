@@ -13,8 +13,10 @@ static_assert(sizeof(AnchorRec) + sizeof(AnchorExt) == 400,
 
 namespace {
 
-// One thread per (tile, transmitter); the block's records are built in
-// shared memory and stored contiguously.
+// One block per anchor group (lpk_split.cuh): up to 32 tiles (one per
+// lane) of up to 4 transmitters (one per warp); the band is a kernel
+// parameter, the group's transmitters are staged in shared memory, and the
+// records go out tile-major through shared memory.
 // MOV: the band's receiver is on an orbit (compiled apart, as the fan-out).
 template <bool MOV>
 __global__ void __launch_bounds__(kAnchorThreads, LPK_ANCHOR_MINB)
@@ -22,16 +24,23 @@ k_split_anchor(const DevBand b, const DevTx *__restrict__ txs, const int32_t *__
                int64_t t0, int64_t n_tiles, int32_t tile_len, AnchorRec *__restrict__ recs,
                AnchorExt *__restrict__ exts) {
     __shared__ __align__(16) AnchorRec srec[kAnchorThreads];
-    const int64_t base = (int64_t)blockIdx.x * kAnchorThreads, total = n_tiles * n_active;
-    const int64_t id = base + threadIdx.x;
-    if (id < total) {
-        const int64_t tile = id / n_active;
-        const int k = (int)(id - tile * n_active);
+    __shared__ __align__(16) DevTx stx[kAnchorGroupTx];
+    const int64_t ntg = (n_tiles + kAnchorGroupTiles - 1) / kAnchorGroupTiles;
+    const int64_t tile0 = (int64_t)(blockIdx.x % ntg) * kAnchorGroupTiles;
+    const int k0 = (int)(blockIdx.x / ntg) * kAnchorGroupTx;
+    const int nt = (int)(n_tiles - tile0 < kAnchorGroupTiles ? n_tiles - tile0 : kAnchorGroupTiles);
+    const int nk = n_active - k0 < kAnchorGroupTx ? n_active - k0 : kAnchorGroupTx;
+    stage_group_txs(txs, active + k0, nk, stx);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane < nt && w < nk) {
+        const int64_t tile = tile0 + lane;
         const int64_t gs = (t0 + tile) * tile_len;  // absolute sample indices of the tile
-        fit_anchor<MOV>(b, txs[active[k]], gs, gs + tile_len - 1, false, srec[threadIdx.x], exts + id);
+        fit_anchor<MOV>(b, stx[w], gs, gs + tile_len - 1, false, srec[lane * kAnchorGroupTx + w],
+                        exts + tile * n_active + k0 + w);
     }
     __syncthreads();
-    store_recs(srec, recs + base, (int)(total - base < kAnchorThreads ? total - base : kAnchorThreads));
+    store_group(srec, recs + tile0 * n_active + k0, nt, nk, n_active);
 }
 
 // One block per tile. MOV: the band's receiver is on an orbit (compiled
@@ -97,8 +106,10 @@ cudaError_t launch_split_anchor(int variant, const DevBand &b, const DevTx *d_tx
     if (na <= 0) return cudaSuccess;
     AnchorRec *recs = (AnchorRec *)d_recs;
     AnchorExt *exts = (AnchorExt *)(recs + na);  // 16-byte aligned: sizeof(AnchorRec) is a multiple of 16
+    const int64_t groups = (n_tiles + kAnchorGroupTiles - 1) / kAnchorGroupTiles *
+                           ((n_active + kAnchorGroupTx - 1) / kAnchorGroupTx);
     (b.rx_kind == LPK_RX_KEPLER ? k_split_anchor<true> : k_split_anchor<false>)<<<
-        (unsigned)((na + kAnchorThreads - 1) / kAnchorThreads), kAnchorThreads, 0, s>>>(
+        (unsigned)groups, kAnchorThreads, 0, s>>>(
         b, d_tx, d_active, n_active, t0, n_tiles, sh.tile, recs, exts);
     return cudaGetLastError();
 }

@@ -168,13 +168,38 @@ __device__ __forceinline__ double iterate_unrounded(const DevTx &tx, double tu, 
     return r * inv_c;
 }
 
-// Copy n records from shared to global memory in 16-byte words, coalesced
-// (every thread of the block takes part).
-__device__ __forceinline__ void store_recs(const AnchorRec *__restrict__ s, AnchorRec *__restrict__ g, int n) {
-    const int4 *src = reinterpret_cast<const int4 *>(s);
-    int4 *dst = reinterpret_cast<int4 *>(g);
-    const int words = n * (int)(sizeof(AnchorRec) / 16);
-    for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+// Anchor groups. An anchor block fits up to kAnchorGroupTiles consecutive
+// tiles (one per lane) of up to kAnchorGroupTx consecutive transmitters
+// (one per warp) of one band: each warp works on one transmitter, whose
+// record and trajectory points it shares, with the band and the
+// transmitters staged in shared memory. Records are stored tile-major, the
+// order the fan-out stages them in.
+constexpr int kAnchorGroupTiles = 32;
+constexpr int kAnchorGroupTx = kAnchorThreads / 32;
+
+// Stage the group's nk transmitters active[0..nk) into stx (all threads).
+__device__ __forceinline__ void stage_group_txs(const DevTx *__restrict__ txs, const int32_t *__restrict__ active,
+                                                int nk, DevTx *stx) {
+    constexpr int wt = (int)(sizeof(DevTx) / 8);
+    for (int i = threadIdx.x; i < nk * wt; i += blockDim.x) {
+        const int k = i / wt;
+        reinterpret_cast<uint64_t *>(stx + k)[i - k * wt] =
+            reinterpret_cast<const uint64_t *>(txs + active[k])[i - k * wt];
+    }
+}
+
+// Store the group's nt x nk records from shared memory (slot l * kAnchorGroupTx
+// + j for tile l, transmitter j) to dst[l * n_active + j], coalesced within
+// each tile's run (all threads).
+__device__ __forceinline__ void store_group(const AnchorRec *srec, AnchorRec *__restrict__ dst, int nt, int nk,
+                                            int n_active) {
+    constexpr int wr = (int)(sizeof(AnchorRec) / 16);
+    const int run = nk * wr;
+    for (int i = threadIdx.x; i < nt * run; i += blockDim.x) {
+        const int l = i / run, r = i - l * run;
+        reinterpret_cast<int4 *>(dst + (int64_t)l * n_active)[r] =
+            reinterpret_cast<const int4 *>(srec + l * kAnchorGroupTx)[r];
+    }
 }
 
 // Newton form of the quadratic through (0, v0), (h, v1), (2h, v2); ih = 1/h.
