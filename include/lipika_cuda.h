@@ -237,7 +237,7 @@ lpk_status lpk_sync(lpk_ctx *ctx);
 
 /* Accuracy of the split-precision fan-out (no reference counterpart; the
  * reference has one all-FP64 path). Renders band samples [i0, i0 + n) of a
- * band with solver LPK_SOLVER_SPLIT and a stationary receiver exactly as
+ * band with solver LPK_SOLVER_SPLIT and a stationary or orbiting receiver exactly as
  * lpk_band_chunk_device does (into d_out, DEVICE memory, when not NULL),
  * and for every (sample, transmitter) the split path evaluates on its fast
  * path also runs the reference-exact FP64 solve and phase (the arithmetic
@@ -257,12 +257,13 @@ lpk_status lpk_split_accuracy(lpk_ctx *ctx, const lpk_band_desc *band, const int
  * file-scope static device array of 22.6 MiB that every GPU loading this
  * library holds until exit. It runs the kernels lpk_band_chunk_device runs
  * for the band's solver (the split path for LPK_SOLVER_SPLIT with a
- * stationary receiver, the FP64 kernel otherwise) on the same inputs, so
+ * stationary or orbiting receiver, the FP64 kernel otherwise) on the same
+ * inputs, so
  * its outputs equal lpk_band_chunk_device's bit for bit. Limits: at most
  * 256 active transmitters; with LPK_CLOCK_DEVICE_WALK a chunk may span at
  * most 2^20 master-clock samples and lie within the first 2^29; a split
- * chunk may need at most 32,768 (tile, transmitter) anchor records (larger
- * requests return LPK_EINVAL). Every call rebuilds the clock walk's block
+ * chunk may need at most 32,768 (tile, transmitter) anchor records and at
+ * most 8,192 flicker-track points (larger requests return LPK_EINVAL). Every call rebuilds the clock walk's block
  * totals and carries from master sample 0, so its walk work grows with the
  * chunk's master-sample offset. The first call on a device looks up the
  * array's address (cudaGetSymbolAddress) — make that first call before any
@@ -331,8 +332,9 @@ int32_t lpk_ctx_split_variant(const lpk_ctx *ctx);
  * that pulls tiles of every unit from a shared counter); the graph is built
  * once and replayed. Outputs equal the single-band entry points' for the
  * same solver and split launch shape (chunk invariance).
- * Units need a stationary receiver (rx_kind LPK_RX_STATIONARY) and a clock
- * mode of LPK_CLOCK_DETERMINISTIC or LPK_CLOCK_DEVICE_WALK; units whose
+ * Units need a stationary or orbiting receiver (rx_kind LPK_RX_STATIONARY
+ * or LPK_RX_KEPLER) and a clock mode of LPK_CLOCK_DETERMINISTIC or
+ * LPK_CLOCK_DEVICE_WALK (with or without a flicker track); units whose
  * clock seed, master rate and Allan deviation agree share one walk (the
  * bands of one receiver). Units with solver LPK_SOLVER_REFERENCE take the
  * reference-exact path for every sample. */
@@ -508,10 +510,11 @@ typedef struct lpk_band_result {
 enum {
     LPK_NOISE_OFF = 0,          /* no AWGN (deterministic comparisons) */
     LPK_NOISE_ON = 1,           /* AWGN at the band's noise power */
-    LPK_GEN_DEVICE_CLOCK = 2,   /* white-FM walk generated on the GPU (counter-based,
-                                   moment-matched) instead of the host stream */
+    LPK_GEN_DEVICE_CLOCK = 2,   /* receiver clock on the GPU (white-FM walk counter-based and
+                                   moment-matched, flicker track from the host stream) instead
+                                   of the host stream; not for host-computed receiver positions */
     LPK_GEN_SPLIT = 4           /* split-precision fan-out (LPK_SOLVER_SPLIT) where the
-                                   band allows it (stationary receiver) */
+                                   band allows it (stationary or orbiting receiver) */
 };
 
 /* generate_band (src/pipeline.rs:836-1019) on the GPU: the chunk loop with
@@ -534,8 +537,9 @@ lpk_status lpk_generate_band_to_file(lpk_scene *s, int32_t r_idx, int32_t b_idx,
  * run_scene_to_dir, src/pipeline.rs:460-536, with the per-unit
  * generate_band calls fused): rounds of round_s seconds, each work unit's
  * chunk handed to sink(user, work_idx, chunk, n) in order. Work units whose
- * receiver moves or whose clock has flicker are rendered by
- * lpk_generate_band instead, after the batch. Flags as lpk_generate_band,
+ * clock stays on the host stream (no LPK_GEN_DEVICE_CLOCK) or whose receiver
+ * positions the host computes are rendered by lpk_generate_band instead,
+ * after the batch. Flags as lpk_generate_band,
  * plus LPK_GEN_AUTOTUNE (tune the launch shape on the middle round first). */
 enum { LPK_GEN_AUTOTUNE = 8 };
 lpk_status lpk_generate_scene(lpk_scene *s, uint64_t seed_base, double round_s, int32_t flags,
