@@ -76,7 +76,7 @@ def _args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--plain-steps", type=int, default=1, help="steps of the plain FP64 paths (0: skip)")
     p.add_argument("--round-s", type=float, default=10.0, help="seconds of scene time per batch round")
-    p.add_argument("--e2e-round-s", type=float, default=4.0,
+    p.add_argument("--e2e-round-s", type=float, default=2.0,
                    help="seconds per round of the e2e leg (shorter rounds overlap more of the copy-out)")
     p.add_argument("--no-autotune", action="store_true", help="keep the default split launch shape")
     p.add_argument("--no-secondary", action="store_true", help="skip the other benchmark scenes")
