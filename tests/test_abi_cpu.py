@@ -178,6 +178,25 @@ def test_band_desc_carries_the_scene_flicker_track():
     assert C.addressof(desc().flicker_delta_s.contents) == C.addressof(d.flicker_delta_s.contents)  # one track
 
 
+def test_band_desc_receiver_kinds():
+    """A circular Keplerian receiver is positioned on the device
+    (LPK_RX_KEPLER, its elements in the descriptor); a stationary one keeps
+    its ECEF position."""
+    from lipika_b200 import workloads as W
+    sc = scenes.config_c1(duration_s=1.0)
+    sc.receivers.append(cfg.Receiver("leo", W._kepler(7_000_000.0, 45.0, 10.0, 20.0), cfg.Clock(),
+                                     [cfg.Band("l1", 1575.42e6, 2.048e6, 290.0, None)]))
+    hs = HostScene(sc)
+    d = N.BandDesc()
+    N.check(N.lib().lpk_scene_band_desc(hs.h, 0, 0, 2026, 0, C.byref(d)))
+    assert d.rx_kind == N.LPK_RX_STATIONARY
+    N.check(N.lib().lpk_scene_band_desc(hs.h, 1, 0, 2026, 2, C.byref(d)))
+    assert d.rx_kind == N.LPK_RX_KEPLER
+    o = d.rx_orbit
+    assert (o.semi_major_axis_m, o.inclination_deg, o.raan_deg, o.true_anomaly_deg_at_epoch) == (
+        7_000_000.0, 45.0, 10.0, 20.0)
+
+
 def test_host_clock_with_flicker_matches_oracle():
     spec = A.ClockCfg(0.0, 1e-10, 0.0, 0.0)
     L = N.lib()

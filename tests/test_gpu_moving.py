@@ -107,3 +107,40 @@ def test_moving_receiver_split_chunk_invariant(ctx):
     assert outs[0].tobytes() == outs[1].tobytes()
     prep.close()
 
+
+
+def test_mixed_batch_stationary_and_orbiting_receivers(ctx):
+    """One batch holding a stationary and an orbiting receiver (the batch then
+    runs its orbit-capable kernels, which take the stationary receiver's
+    tiles down the stationary code): every unit within 1e-5 of the oracle,
+    and the stationary receiver's output equal bit for bit to the same
+    receiver batched alone."""
+    import copy
+    sc = W.config_c1(duration_s=0.2, noise=False,
+                     clock=cfg.Clock(frequency_offset_y0=0.4e-6, initial_time_offset_s=2e-8))
+    moving = copy.deepcopy(sc.receivers[0])
+    moving.name = "leo_rx"
+    moving.trajectory = W._kepler(6_900_000.0, 60.0, 30.0, 100.0)
+    sc.receivers.append(moving)
+    prep = P.Prepared(sc, ctx)
+    parts: dict = {}
+    prep.generate_scene(2026, 0.1, lambda w, c: parts.setdefault(w, []).append(c) and False, noise=False,
+                        device_clock=True, split=True)
+    osc = O.Scene(sc)
+    kinds = set()
+    for w, (r, b) in enumerate(prep.work()):
+        kinds.add(prep.band_desc(r, b, 2026, w).rx_kind)
+        got = np.concatenate(parts[w])
+        ref = osc.generate_band(r, b, 2026, w, 1 << 20, 4, O.NOISE_NONE)["iq"]
+        assert _rel(got, ref) <= IQ_RTOL, (w, _rel(got, ref))
+    assert kinds == {N.LPK_RX_STATIONARY, N.LPK_RX_KEPLER}
+    prep.close()
+    alone = W.config_c1(duration_s=0.2, noise=False,
+                        clock=cfg.Clock(frequency_offset_y0=0.4e-6, initial_time_offset_s=2e-8))
+    p2 = P.Prepared(alone, ctx)
+    solo: dict = {}
+    p2.generate_scene(2026, 0.1, lambda w, c: solo.setdefault(w, []).append(c) and False, noise=False,
+                      device_clock=True, split=True)
+    for w in solo:  # the stationary receiver's units come first in both scenes
+        assert np.concatenate(solo[w]).tobytes() == np.concatenate(parts[w]).tobytes()
+    p2.close()
