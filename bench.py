@@ -535,8 +535,9 @@ def run_ours(a):
     plain, fp64_paths = None, None
     if a.plain_steps > 0:
         plain, fp64_paths = _plain_fp64(rig, units, total_txrx, a.round_s, a.plain_steps, a.chunk)
-        plain["value"] *= ws
-        for v in fp64_paths.values():
+        for v in [plain] + list(fp64_paths.values()):
+            # the same algorithmic basis as the roofline: 76 flop per tx·rx sample on one GPU
+            v["fp64_frac"] = FLOP_PER_SAMPLE * v["value"] / 1e12 / peak_fp64.value if peak_fp64.value else None
             v["value"] *= ws
     split_band = None
     if a.plain_steps > 0 and ws == 1:
