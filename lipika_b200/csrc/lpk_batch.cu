@@ -191,10 +191,11 @@ k_batch_anchor(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ 
 }
 
 // The persistent fan-out: blocks take tiles from the round's counter until
-// none is left, claiming the next tile while they work on the current one
-// (the claim's latency is hidden and the end-of-tile barrier publishes it).
-// A block restages the band and its transmitters only when the next tile
-// belongs to another unit.
+// none is left, claiming two tiles ahead (the claim's latency is hidden and
+// the end-of-tile barrier publishes it), so one lane can ask for the next
+// tile's anchor records to be brought into L2 while the current tile
+// renders. A block restages the band and its transmitters only when the next
+// tile belongs to another unit.
 // MOV: some unit's receiver is on an orbit; its tiles take the orbit-aware
 // tile code (compiled apart, so batches of stationary receivers run kernels
 // without it).
@@ -209,15 +210,27 @@ k_batch_fanout(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ 
     DevTx *stx = reinterpret_cast<DevTx *>(smem_raw + ((sizeof(DevBand) + 15) / 16) * 16);
     AnchorRec *srec = reinterpret_cast<AnchorRec *>(reinterpret_cast<unsigned char *>(stx) +
                                                     sizeof(DevTx) * (size_t)max_active);
-    __shared__ unsigned long long s_next[2];
+    __shared__ unsigned long long s_next[3];  // tiles it, it + 1 (published) and it + 2 (being claimed)
     int cur = -1;
     const int64_t total = rd->total_tiles;
-    if (threadIdx.x == 0) s_next[0] = atomicAdd(counter, 1ull);
+    if (threadIdx.x == 0) {
+        s_next[0] = atomicAdd(counter, 1ull);
+        s_next[1] = atomicAdd(counter, 1ull);
+    }
     __syncthreads();
-    for (int it = 0;; it ^= 1) {
-        const int64_t g = (int64_t)s_next[it];
+    for (int it = 0;; ++it) {
+        const int64_t g = (int64_t)s_next[it % 3];
         if (g >= total) break;
-        if (threadIdx.x == 0) s_next[it ^ 1] = atomicAdd(counter, 1ull);  // read after the end-of-tile barrier
+        if (threadIdx.x == 0) s_next[(it + 2) % 3] = atomicAdd(counter, 1ull);  // read after the end-of-tile barrier
+        if (threadIdx.x == 32) {  // the next tile's records into L2 while this tile renders (no completion to wait on)
+            const int64_t gn = (int64_t)s_next[(it + 1) % 3];
+            if (gn < total) {
+                const RoundUnit &rn = rd->s[find_slot_tiles(*rd, gn)];
+                const int na = units[rn.unit].n_active;
+                if (na > 0)
+                    prefetch_l2(recs + rn.rec_off + (gn - rn.tile_off) * na, (uint32_t)(sizeof(AnchorRec) * na));
+            }
+        }
         const int sl = find_slot_tiles(*rd, g);
         const RoundUnit &ru = rd->s[sl];
         const BatchUnit bu = units[ru.unit];

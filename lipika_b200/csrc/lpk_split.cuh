@@ -932,6 +932,12 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
     }
 }
 
+// Ask for `bytes` (a multiple of 16, from a 16-byte aligned address) of
+// global memory to be brought into L2; nothing waits for it (a hint).
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 // Stage the tile's transmitters and anchor records into shared memory
 // (8-byte words, all threads of the block).
 __device__ __forceinline__ void stage_tile(const DevTx *__restrict__ txs, const int32_t *__restrict__ active,
