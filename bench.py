@@ -612,7 +612,7 @@ def run_ours(a):
     secondary = None
     if ws == 1 and not a.no_secondary:
         secondary = {}
-        for name, rs, st in (("c1", 30.0, 3), ("c2", 2.0, 2), ("c3", 30.0, 2)):
+        for name, rs, st in (("c1", 60.0, 3), ("c2", 2.0, 2), ("c3", 30.0, 2)):
             if name != a.scene:
                 secondary[name] = _secondary(rig, name, seed, rs, st, a.chunk)
 
