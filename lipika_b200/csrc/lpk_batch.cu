@@ -58,7 +58,7 @@ struct RoundWalk {
     int64_t g_known;        // groups whose sums are stored before the round
 };
 struct RoundDesc {
-    int64_t total_tiles, total_recs, total_groups, total_walk_blocks;
+    int64_t total_tiles, total_groups, total_walk_blocks;
     int32_t n_slots, n_walks, tile, parity;  // parity: which output buffer the round writes
     int64_t wb_off[kMaxWalks + 1];  // prefix of scanned blocks per walk
     RoundWalk w[kMaxWalks];
@@ -399,7 +399,6 @@ void plan_round(lpk_batch *b, int64_t round, int tile, RoundDesc &rd, bool commi
     }
     rd.n_slots = (int32_t)order.size();
     rd.total_tiles = tiles;
-    rd.total_recs = recs;
     rd.total_groups = groups;
     rd.n_walks = (int32_t)b->walks.size();
     int64_t wb = 0, partial_blocks = 0;
@@ -460,8 +459,8 @@ lpk_status build_graph(lpk_batch *b, int p) {
     cudaMemcpyAsync(b->d_round, b->h_round[p], sizeof(RoundDesc), cudaMemcpyHostToDevice, c->stream);
     cudaEventRecord(b->fork, c->stream);
     cudaStreamWaitEvent(b->side, b->fork, 0);
-    (b->any_orbit ? k_batch_anchor<true> : k_batch_anchor<false>)<<<b->anchor_grid, kAnchorThreads, 0, b->side>>>(b->d_bands, b->d_units, c->d_tx, b->d_act, b->d_round,
-                                                        b->d_recs, b->d_exts);
+    (b->any_orbit ? k_batch_anchor<true> : k_batch_anchor<false>)<<<b->anchor_grid, kAnchorThreads, 0, b->side>>>(
+        b->d_bands, b->d_units, c->d_tx, b->d_act, b->d_round, b->d_recs, b->d_exts);
     cudaEventRecord(b->join, b->side);
     if (!b->walks.empty()) {
         k_batch_walk<<<b->walk_grid, kWalkThreads, 0, c->stream>>>(b->d_walks, b->d_round);
