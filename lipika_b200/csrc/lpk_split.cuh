@@ -744,6 +744,14 @@ __device__ __forceinline__ void split_pass(const DevTx &tx, const AnchorRec &R, 
     }
 }
 
+// The exact path's contribution (rare samples and whole exact tiles), out of
+// line so the reference arithmetic's registers stay out of the fast loop's.
+static __device__ __noinline__ bool exact_contribution(const DevTx &tx, const DevBand &b, double t_local, double tu,
+                                                double delta, double ox, double oy, double oz, float &cr, float &ci,
+                                                double *ph, double *te, double *rg) {
+    return contribution(tx, b, t_local, tu, delta, ox, oy, oz, cr, ci, ph, te, rg);
+}
+
 // One tile of S * THREADS band samples starting at chunk index `first`,
 // with the tile's transmitters and anchor records staged in shared memory.
 // Samples outside [0, b.n) are skipped; the transmitters are summed in
@@ -880,7 +888,7 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
             sample_clock<THREADS>(b, first, s, rfs, tl, dl);
             double ox = b.rx[0], oy = b.rx[1], oz = b.rx[2];
             if constexpr (MOV) band_rx(b, 0, sc[s].tu, ox, oy, oz);
-            const bool on = contribution(T, b, tl, sc[s].tu, dl, ox, oy, oz, cr, ci, &ph, &te, &rg);
+            const bool on = exact_contribution(T, b, tl, sc[s].tu, dl, ox, oy, oz, cr, ci, &ph, &te, &rg);
             if constexpr (UNOCC) {
                 if (on && !gate_off) atomicOr(b.unocc_words + k, 1u);
             } else {
