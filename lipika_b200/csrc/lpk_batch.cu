@@ -198,8 +198,10 @@ k_batch_anchor(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ 
 // tile belongs to another unit.
 // MOV: some unit's receiver is on an orbit; its tiles take the orbit-aware
 // tile code (compiled apart, so batches of stationary receivers run kernels
-// without it).
-template <int TILE, int THREADS, int MINB, bool MOV>
+// without it). OOL: the exact path is an out-of-line call (batches with a
+// split unit, whose exact samples are rare; a batch of reference-solver units
+// only keeps it inline).
+template <int TILE, int THREADS, int MINB, bool MOV, bool OOL>
 __global__ void __launch_bounds__(THREADS, MINB)
 k_batch_fanout(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ units,
                const DevTx *__restrict__ txs, const int32_t *__restrict__ act, const DevWalk *__restrict__ walks,
@@ -253,13 +255,11 @@ k_batch_fanout(const DevBand *__restrict__ bands, const BatchUnit *__restrict__ 
         const int64_t first = (ru.t0 + local) * TILE - ru.i0;
         const AnchorExt *xrec = exts + ru.rec_off + local * bu.n_active;
         if (MOV && sb->rx_kind == LPK_RX_KEPLER)  // block-uniform
-            split_tile<TILE / THREADS, THREADS, false, false, false, true>(*sb, stx, srec, xrec, bu.n_active, first,
-                                                                           bu.out[rd->parity], nullptr, nullptr,
-                                                                           nullptr);
+            split_tile<TILE / THREADS, THREADS, false, false, false, true, OOL>(
+                *sb, stx, srec, xrec, bu.n_active, first, bu.out[rd->parity], nullptr, nullptr, nullptr);
         else
-            split_tile<TILE / THREADS, THREADS, false, false, false, false>(*sb, stx, srec, xrec, bu.n_active, first,
-                                                                            bu.out[rd->parity], nullptr, nullptr,
-                                                                            nullptr);
+            split_tile<TILE / THREADS, THREADS, false, false, false, false, OOL>(
+                *sb, stx, srec, xrec, bu.n_active, first, bu.out[rd->parity], nullptr, nullptr, nullptr);
         __syncthreads();  // the next stage overwrites the shared tiles
     }
 }
@@ -270,9 +270,11 @@ using FanoutKernel = void (*)(const DevBand *, const BatchUnit *, const DevTx *,
 
 struct FanoutShape {
     int tile, threads;
-    FanoutKernel kern[2];  // [some receiver on an orbit]
+    FanoutKernel kern[2][2];  // [some receiver on an orbit][some unit on the split solver]
 };
-#define LPK_BATCH_ENTRY(I, T, N, M) {T, N, {k_batch_fanout<T, N, M, false>, k_batch_fanout<T, N, M, true>}},
+#define LPK_BATCH_ENTRY(I, T, N, M)                                                                    \
+    {T, N, {{k_batch_fanout<T, N, M, false, false>, k_batch_fanout<T, N, M, false, true>},           \
+            {k_batch_fanout<T, N, M, true, false>, k_batch_fanout<T, N, M, true, true>}}},
 const FanoutShape kFanout[kSplitVariants] = {LPK_SPLIT_VARIANTS(LPK_BATCH_ENTRY)};
 #undef LPK_BATCH_ENTRY
 
@@ -325,6 +327,7 @@ struct lpk_batch {
     int64_t n_rounds = 0;
     int32_t max_active = 0;
     int any_orbit = 0;                              // some unit's receiver is on an orbit
+    int any_split = 0;                              // some unit takes the split solver
     int variant = 0, bps = 0, max_bps = 0, walk_grid = 0, anchor_grid = 0;
     cudaGraph_t graph_src[2] = {nullptr, nullptr};
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -447,7 +450,7 @@ lpk_status build_graph(lpk_batch *b, int p) {
     lpk_ctx *c = b->ctx;
     const FanoutShape &sh = kFanout[b->variant];
     const size_t smem = fanout_smem(b->max_active);
-    const FanoutKernel kern = sh.kern[b->any_orbit];
+    const FanoutKernel kern = sh.kern[b->any_orbit][b->any_split];
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_fail(c, e, "batch fan-out shared memory");
     int dev_sms = 0;
@@ -514,7 +517,7 @@ lpk_status configure(lpk_batch *b, int variant, int bps) {
     if (variant < 0 || variant >= kSplitVariants) return fail(b->ctx, LPK_EINVAL, "unknown split variant");
     const FanoutShape &sh = kFanout[variant];
     const size_t smem = fanout_smem(b->max_active);
-    const FanoutKernel kern = sh.kern[b->any_orbit];
+    const FanoutKernel kern = sh.kern[b->any_orbit][b->any_split];
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_fail(b->ctx, e, "batch fan-out shared memory");
     int occ = 0;
@@ -650,6 +653,7 @@ lpk_status lpk_batch_create(lpk_ctx *c, const lpk_work_unit *wu, int32_t n_units
         for (int k = 0; k < w.n_active; ++k) h_act.push_back(w.active[k]);
         b->max_active = std::max(b->max_active, w.n_active);
         if (w.band.rx_kind == LPK_RX_KEPLER) b->any_orbit = 1;
+        if (w.band.solver == LPK_SOLVER_SPLIT) b->any_split = 1;
         b->units.push_back(uh);
         b->h_units.push_back(bu);
     }

@@ -764,7 +764,10 @@ static __device__ __noinline__ bool exact_contribution(const DevTx &tx, const De
 // counts are added to b.acc_stats[2..3].
 // MOV: the band's receiver is on an orbit (see split_pass); its horizon gate
 // is off (an optimisation only: the gated samples are zero either way).
-template <int S, int THREADS, bool DBG, bool UNOCC, bool ACC, bool MOV>
+// OOL: the exact path's contribution is an out-of-line call (for fan-outs
+// whose exact samples are rare: the reference arithmetic's registers stay
+// out of the fast loop's allocation); inline otherwise.
+template <int S, int THREADS, bool DBG, bool UNOCC, bool ACC, bool MOV, bool OOL = false>
 // xrec: the tile's AnchorExt records in global memory (index k per
 // transmitter), read only for tiles that cross more than one grid node.
 __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, const AnchorRec *srec,
@@ -888,7 +891,9 @@ __device__ __forceinline__ void split_tile(const DevBand &b, const DevTx *stx, c
             sample_clock<THREADS>(b, first, s, rfs, tl, dl);
             double ox = b.rx[0], oy = b.rx[1], oz = b.rx[2];
             if constexpr (MOV) band_rx(b, 0, sc[s].tu, ox, oy, oz);
-            const bool on = exact_contribution(T, b, tl, sc[s].tu, dl, ox, oy, oz, cr, ci, &ph, &te, &rg);
+            bool on;
+            if constexpr (OOL) on = exact_contribution(T, b, tl, sc[s].tu, dl, ox, oy, oz, cr, ci, &ph, &te, &rg);
+            else on = contribution(T, b, tl, sc[s].tu, dl, ox, oy, oz, cr, ci, &ph, &te, &rg);
             if constexpr (UNOCC) {
                 if (on && !gate_off) atomicOr(b.unocc_words + k, 1u);
             } else {
